@@ -1,0 +1,383 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the continuous-subgraph-matching hot path.
+
+Workload (default): the 2^22-vertex RMAT graph (average degree 28, 16 vertex
+labels Zipf(1.2), 4 edge labels) with a 16-vertex dense query (>= 32 edges)
+and an 80/20 insert/delete edge stream, per-update cap 10^6 matches (the
+reference's --max-results), run by the SymBi plugin.  A step is one batch of
+65,536 stream updates.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is batched updates/s with the stream
+already in HBM (CUDA events on the engine's stream); `e2e` is the same metric
+through the C ABI with pinned host buffers, the host->device copy of each
+step's updates and the device->host read of its results inside the timed
+region.  The plain one-update-per-launch form is measured on a sample of the
+same stream from the same initial graph and must give identical counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact counts"
+
+CONFIGS = {
+    "c3": {
+        "preset": "c3", "algo": "parallel_symbi", "batch": 65536, "max_results": 1_000_000,
+        "min_updates": 1_000_000,
+        "workload": "RMAT 2^22 V, avg deg 28 (58.7M edges), 16 vlabels Zipf(1.2), 4 elabels; 16-vertex dense "
+                    "query (avg deg >= 4); edge stream 80% insert / 20% delete; max_results 1e6 per update",
+    },
+    "c2": {
+        "preset": "c2", "algo": "parallel_turboflux", "batch": 65536, "max_results": 1_000_000,
+        "min_updates": 100_000,
+        "workload": "RMAT 2^19 V, avg deg 16, 8 vlabels Zipf(1.0), 2 elabels; 8-vertex sparse query; "
+                    "edge stream 90% insert / 10% delete; max_results 1e6 per update",
+    },
+    "c1": {
+        "preset": "c1", "algo": "parallel_graphflow", "batch": 2000, "max_results": 0, "min_updates": 2000,
+        "workload": "RMAT 2^14 V, avg deg 8, 4 vlabels, 1 elabel; 6-vertex induced query; 2,000 insertions",
+    },
+}
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_QUERY}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cuda_view(ptr: int, nbytes: int, device: int):
+    """torch uint8 view of raw device memory (no copy)."""
+    import torch
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Arr(), device=f"cuda:{device}")
+
+
+def get_workload(cfg: dict, n_updates: int):
+    from paracosm_b200 import workload
+    base = Path(os.environ.get("CSM_BENCH_DIR", "/tmp/csm_bench"))
+    d = base / f"{cfg['preset']}_{n_updates}"
+    t0 = time.perf_counter()
+    w = workload.generate(cfg["preset"], d, updates=n_updates)
+    log(f"workload {d} ready in {time.perf_counter() - t0:.1f}s: {len(w.vlabels)} V, {len(w.edges)} E, "
+        f"{len(w.stream)} updates")
+    return w
+
+
+def ref_sample(w, algo: str, threads: int, cap: int, budget_s: float, hard_timeout: float, skip: int = 0):
+    """Times the reference (oracle/_ref, built from the reference sources) on a bounded
+    prefix of the stream: per-update latencies of the plugin calls."""
+    drv = ROOT / "oracle" / "_ref" / "ref_driver"
+    if not drv.exists():
+        return None, "reference driver not built (oracle/_ref/ref_driver)"
+    out = Path(tempfile.mkdtemp()) / "ref.csv"
+    cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(w.directory / "data.bin"), "-U",
+           str(w.directory / "stream.bin"), "-a", algo, "-t", str(threads), "--time-budget", str(budget_s),
+           "--out", str(out)]
+    if cap:
+        cmd += ["--max-results", str(cap)]
+    t0 = time.perf_counter()
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=hard_timeout)
+        note = "" if r.returncode == 0 else f"exit {r.returncode}"
+    except subprocess.TimeoutExpired:
+        note = f"killed after {hard_timeout:.0f}s (an update ran past the sample budget)"
+    wall = time.perf_counter() - t0
+    if not out.exists():
+        return None, f"no output ({note})"
+    lat = []
+    for line in out.read_text().splitlines()[1:]:
+        parts = line.split(",")
+        if len(parts) >= 10:
+            lat.append(int(parts[8]))
+    lat = np.array(lat[skip:], dtype=np.float64)
+    if len(lat) == 0:
+        return None, f"no update finished ({note})"
+    return {"updates": int(len(lat)), "seconds": float(lat.sum() / 1e9),
+            "value": float(len(lat) / (lat.sum() / 1e9)), "p50_ns": float(np.percentile(lat, 50)),
+            "p99_ns": float(np.percentile(lat, 99)), "wall_s": wall, "note": note}, None
+
+
+def run_reference_arm(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps_upd = 64  # one reference step = 64 stream updates
+    n_updates = max(cfg["min_updates"], (args.warmup + args.steps + 4) * cfg["batch"])
+    w = get_workload(cfg, n_updates)
+    threads = os.cpu_count() or 1
+    budget = float(os.environ.get("CSM_REF_BUDGET_S", "60"))
+    res, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], budget, budget + 600,
+                          skip=args.warmup * steps_upd)
+    line = {"impl": "reference", "metric": METRIC, "unit": "updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "dtype": "u32", "data": "synthetic", "config": {"workload": cfg["workload"]}}
+    if res is None:
+        line.update({"value": None, "unavailable": err})
+    else:
+        line.update({"value": res["value"], "ms_per_step": 1000.0 * steps_upd / res["value"],
+                     "p50_us": res["p50_ns"] / 1e3, "p99_us": res["p99_ns"] / 1e3,
+                     "cpu_baseline": {"value": res["value"], "unit": "updates/s", "cores": threads,
+                                      "kind": "reference",
+                                      "sample": f"first {res['updates']} timed updates of the stream after "
+                                                f"{args.warmup * steps_upd} warm-up updates, "
+                                                f"parallel_turboflux -t {threads}, {budget:.0f}s budget "
+                                                f"{res['note']}".strip()},
+                     "e2e": {"value": res["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c3")
+    ap.add_argument("--algo", default=None)
+    ap.add_argument("--batch", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--plain-sample", type=int, default=3000)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    cfg = dict(CONFIGS[args.config])
+    if args.algo:
+        cfg["algo"] = args.algo
+    if args.batch:
+        cfg["batch"] = args.batch
+    if args.impl == "reference":
+        return run_reference_arm(args, cfg)
+
+    import torch
+    import torch.distributed as dist
+
+    from paracosm_b200 import RESULT_DTYPE, Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = local
+    B, W, K, KE = cfg["batch"], args.warmup, args.steps, args.e2e_steps
+    n_updates = max(cfg["min_updates"], (W + K + KE) * B)
+    w = get_workload(cfg, n_updates)
+    qv, qe = w.queries[0]
+    stream = w.stream
+    assert len(stream) >= (W + K + KE) * B
+
+    # ---- batched engine, inputs resident in HBM ----
+    t0 = time.perf_counter()
+    eng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev)
+    eng.set_query(qv, qe)
+    eng.load_graph(w.vlabels, w.edges)
+    eng.build_index()
+    log(f"engine ready in {time.perf_counter() - t0:.1f}s")
+    d_stream = torch.from_numpy(stream[: (W + K) * B].view(np.uint8).copy()).to(f"cuda:{dev}")
+    ext = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{dev}")
+    res_dev = torch.empty(K * B * RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{dev}")
+    launches0 = None
+    for i in range(W):
+        eng.submit_device(d_stream.data_ptr() + i * B * 16, B)
+        eng.wait()
+    st0 = eng.stats()
+    launches0 = eng.kernel_launches()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        ev0.record(ext)
+        for k in range(K):
+            eng.submit_device(d_stream.data_ptr() + (W + k) * B * 16, B)
+            rp, rn = eng.results_device()
+            with torch.cuda.stream(ext):
+                res_dev[k * B * RESULT_DTYPE.itemsize:(k + 1) * B * RESULT_DTYPE.itemsize].copy_(
+                    cuda_view(rp, rn * RESULT_DTYPE.itemsize, dev))
+        ev1.record(ext)
+        ev1.synchronize()
+        eng.wait()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    st1 = eng.stats()
+    launches = eng.kernel_launches() - launches0
+    res = np.frombuffer(res_dev.cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
+    value = world * K * B / (ms / 1e3)
+    lat = res["latency_ns"].astype(np.float64)
+    search_ms = st1["search_ms"] - st0["search_ms"]
+    search_n = st1["search_launches"] - st0["search_launches"]
+    work = float(res["work_bytes"].sum())
+    peak, peak_kind = measured_peak_hbm()
+    achieved = (work / 1e9) / (search_ms / 1e3) if search_ms > 0 else 0.0
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    host = torch.from_numpy(stream[(W + K) * B:(W + K + KE) * B].view(np.uint8).copy()).pin_memory()
+    e2e_ms = 0.0
+    for k in range(KE):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        first = eng.submit_ptr(host.data_ptr() + k * B * 16, B)
+        r = eng.results(first, B)
+        b.record(ext)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+        assert len(r) == B
+    e2e_value = world * KE * B / (e2e_ms / 1e3) if e2e_ms > 0 else None
+    eng.close()
+
+    # ---- plain form (one update per launch sequence) on a sample, same initial graph ----
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        P = min(args.plain_sample, W * B)
+        peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev)
+        peng.set_query(qv, qe)
+        peng.load_graph(w.vlabels, w.edges)
+        peng.build_index()
+        beng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev)
+        beng.set_query(qv, qe)
+        beng.load_graph(w.vlabels, w.edges)
+        beng.build_index()
+        sample = np.ascontiguousarray(stream[:P])
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        pr = peng.run(sample)
+        plain_s = time.perf_counter() - t1
+        pst = peng.stats()
+        br = beng.run(sample)
+        same = bool(np.array_equal(pr["pos"], br["pos"]) and np.array_equal(pr["neg"], br["neg"]) and
+                    np.array_equal(pr["status"], br["status"]))
+        plain = {"value": P / plain_s, "updates": P, "device_ms": pst["total_device_ms"],
+                 "p50_us": float(np.percentile(np.diff(np.concatenate([[0], pr["latency_ns"]])), 50)) / 1e3,
+                 "counts_equal_batched": same}
+        peng.close()
+        beng.close()
+
+    # ---- CPU baseline: the reference compiled from its sources, bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        r, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], args.cpu_budget,
+                            args.cpu_budget + 400)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": "updates/s", "cores": threads, "kind": "reference",
+                   "sample": f"first {r['updates']} updates of the same stream, parallel_turboflux -t {threads} "
+                             f"(reference sources, sequential update order), {args.cpu_budget:.0f}s budget "
+                             f"{r['note']}".strip(),
+                   "p50_us": r["p50_ns"] / 1e3, "p99_us": r["p99_ns"] / 1e3}
+        else:
+            cpu = {"value": None, "unit": "updates/s", "cores": threads, "kind": "reference", "sample": err}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "plugin": cfg["algo"], "batch": B, "updates_timed": K * B,
+                       "l2": "inputs larger than L2 (graph ~1.2 GB in HBM)", "max_results": cfg["max_results"]},
+            "p50_us": float(np.percentile(lat, 50)) / 1e3, "p99_us": float(np.percentile(lat, 99)) / 1e3,
+            "plain": plain,
+            "batched_over_plain": (value / plain["value"]) if plain else None,
+            "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": B * 16,
+                    "d2h_bytes_per_step": B * RESULT_DTYPE.itemsize},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_kind": peak_kind, "kernel": "k_search", "launches": search_n,
+                         "kernel_ms": search_ms, "algorithmic_bytes": work},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "counts": {"positive": int(res["pos"].sum()), "negative": int(res["neg"].sum()),
+                       "capped": int((res["status"] == 1).sum()), "invalid": int((res["status"] == 3).sum()),
+                       "unsafe": int(((res["pos"] + res["neg"]) > 0).sum())},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/*
+ * csm_gpu.h - C ABI of the B200 continuous-subgraph-matching engine.
+ *
+ * The engine replaces the hot path behind the reference's plugin interface
+ * `class matching` (ParaCOSM/CSM/matching/matching.h:9-66) for the plugins
+ * `parallel_graphflow`, `parallel_turboflux` and `parallel_symbi`
+ * (ParaCOSM/CSM/matching/main.cpp:740-757).  A C++ host (paracosm_b200/host)
+ * wraps these entry points in `matching`-style plugin classes so that the
+ * csm command line and its output lines are unchanged.
+ *
+ * Conventions
+ *   - Every int-returning call returns CSM_OK (0) or a negative CSM_E* code;
+ *     nothing calls exit() (the reference exits on bad input,
+ *     ParaCOSM/CSM/graph/graph.cpp:98-109).  csm_gpu_last_error() gives text.
+ *   - Input buffers are host memory owned by the caller for the duration of
+ *     the call only; the library copies what it keeps.  The *_device variants
+ *     take device pointers instead.
+ *   - One context is used by one host thread at a time.
+ *   - All ids and labels are uint32; counts are uint64.
+ *   - Results keep the sequential update order's semantics
+ *     (ParaCOSM/CSM/matching/main.cpp:628-674): an insertion counts the
+ *     embeddings containing the new edge after adding it, a deletion counts
+ *     them before removing it, and every update sees the graph left by all
+ *     earlier updates, whether updates are run one per launch or batched.
+ */
+#ifndef CSM_GPU_H
+#define CSM_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ---------------------------------------------------- */
+#define CSM_OK 0
+#define CSM_EINVAL -1       /* bad argument */
+#define CSM_ENOMEM -2       /* device memory or HBM budget exhausted */
+#define CSM_ECUDA -3        /* CUDA runtime error */
+#define CSM_ESTATE -4       /* call out of order (e.g. submit before load) */
+#define CSM_EUNSUPPORTED -5 /* input outside the supported limits */
+#define CSM_ETIMEOUT -6     /* csm_gpu_wait deadline passed */
+#define CSM_EDEVICE -7      /* a kernel reported an internal error flag */
+
+/* ---- per-update status (csm_result.status) -------------------------- */
+#define CSM_ST_OK 0         /* exact count */
+#define CSM_ST_CAPPED 1     /* count reached max_results; reported count == max_results */
+#define CSM_ST_TIMED_OUT 2  /* per-update deadline reached; count is a lower bound */
+#define CSM_ST_INVALID 3    /* e.g. deleting a missing edge; count 0, graph unchanged */
+
+/* ---- algorithms (the reference's -a names) -------------------------- */
+#define CSM_ALGO_GRAPHFLOW 0 /* -a parallel_graphflow / graphflow: no index */
+#define CSM_ALGO_TURBOFLUX 1 /* -a parallel_turboflux / turboflux: DCG over a query spanning tree */
+#define CSM_ALGO_SYMBI 2     /* -a parallel_symbi / symbi: DCS over a DAG of all query edges */
+
+/* ---- execution modes ------------------------------------------------ */
+#define CSM_MODE_BATCHED 0   /* many updates per launch sequence (default) */
+#define CSM_MODE_PLAIN 1     /* one update per launch sequence */
+
+typedef struct csm_cfg {
+  int32_t algorithm;          /* CSM_ALGO_* */
+  int32_t homomorphism;       /* != 0: drop the injectivity check (reference --homo) */
+  uint64_t max_results;       /* per-update cap (reference --max-results); 0 = none */
+  uint64_t deadline_ns;       /* per-update time budget on the device; 0 = none */
+  uint64_t hbm_budget_bytes;  /* device memory the context may hold; 0 = 90% of free */
+  int32_t mode;               /* CSM_MODE_* */
+  uint32_t max_batch;         /* updates per batch in CSM_MODE_BATCHED (<= 65536); 0 = 65536 */
+  int32_t want_hash;          /* != 0: compute the per-update match-set hash */
+  int32_t device;             /* CUDA device ordinal */
+  int32_t turboflux_compat;   /* != 0: reproduce the reference TurboFlux deletion count,
+                                 which ignores the anchor edge label
+                                 (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:975) */
+  uint32_t warps_per_block;   /* search kernel tuning; 0 = autotuned */
+  uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
+  uint32_t vlabel_capacity;   /* vertex labels the graph may hold; 0 = max seen at load + 1 */
+  uint32_t elabel_capacity;   /* edge labels the graph may hold; 0 = max seen at load + 1 */
+  uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */
+  uint32_t reserved[5];
+} csm_cfg;
+
+/* Same 16-byte layout as the reference's InsertUnit fields
+ * (ParaCOSM/CSM/utils/types.h:34-42). */
+typedef struct csm_update {
+  uint8_t type;     /* 'v' or 'e' */
+  uint8_t is_add;   /* 1 = insertion, 0 = deletion */
+  uint16_t pad;
+  uint32_t id1, id2, label;
+} csm_update;
+
+typedef struct csm_result {
+  uint64_t pos;     /* positive matches of this update (insertions) */
+  uint64_t neg;     /* negative matches of this update (deletions) */
+  uint64_t hash;    /* order-independent match-set hash (0 unless want_hash and status OK) */
+  uint64_t work_bytes; /* algorithmic bytes: 4 B x the sizes of all back-neighbour segments of
+                          every expanded search-tree node, + 16 B per applied edge mutation */
+  uint64_t latency_ns; /* submit -> result ready, measured on the device clock */
+  uint32_t status;  /* CSM_ST_* */
+  uint32_t safe;    /* 1 when the label-triple test (Classify) found no matching query edge */
+} csm_result;
+
+typedef struct csm_stats {
+  uint64_t num_vertices, num_edges;
+  uint64_t updates_done, vertex_updates, edge_updates;
+  uint64_t positive, negative, unsafe_updates; /* reference summary counters */
+  uint64_t batches, kernel_launches;
+  uint64_t search_tasks, donated_tasks;
+  uint64_t device_bytes;      /* device memory held by the context */
+  uint64_t pool_entries, pool_capacity;
+  double last_batch_ms, total_device_ms;
+  uint64_t index_entries, index_vertices; /* GetMemoryCost analogue */
+  uint64_t search_launches;   /* launches of the search kernel */
+  double search_ms;           /* their summed duration, from CUDA events on the launching stream */
+  uint64_t work_bytes;        /* algorithmic bytes of all completed updates (csm_result.work_bytes) */
+} csm_stats;
+
+typedef struct csm_ctx csm_ctx;
+
+/* Fills *cfg with the defaults. */
+void csm_gpu_default_cfg(csm_cfg* cfg);
+
+/* Creates a context on cfg->device (Parallel_* constructors, main.cpp:740-757). */
+int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out);
+
+/* Sets the query graph: n_qv vertices with labels, n_qe undirected edges as
+ * (u, v, label) triples (Graph::LoadFromFile of -q, graph.cpp:217-249).
+ * Must come before csm_gpu_build_index. */
+int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe,
+                      const uint32_t* q_edges);
+
+/* Loads the initial data graph (-d): n_v vertex slots with labels
+ * (0xffffffff = absent) and n_e undirected edges as (v1, v2, label) triples.
+ * Self loops and repeated edges are dropped (the first label wins). */
+int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint64_t n_e,
+                       const uint32_t* edges);
+
+/* Preprocessing(): matching orders and, for TurboFlux / SymBi, the auxiliary
+ * index (BuildDAG + BuildDCS). */
+int csm_gpu_build_index(csm_ctx* ctx);
+
+/* InitialMatching(): number of embeddings in the current graph. */
+int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count);
+
+/* Classify(v1, v2, label) for n updates: safe_out[i] = 1 when no query edge
+ * matches the label triple (L(v1), L(v2), label) in either orientation
+ * (ParaCOSM/CSM/matching/Parallel_GraphFlow/parallel_graphflow.cpp:1990-2016). */
+int csm_gpu_classify(csm_ctx* ctx, uint64_t n, const csm_update* ups, uint8_t* safe_out);
+
+/* Queues n updates (host memory) after all earlier ones; sequence numbers
+ * continue from the previous submit.  Runs asynchronously. */
+int csm_gpu_submit(csm_ctx* ctx, uint64_t n, const csm_update* ups);
+/* Same, with the updates already in device memory.  Only edge updates are
+ * taken from device memory; a vertex update there is reported
+ * CSM_ST_INVALID (submit vertex updates from host memory). */
+int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups);
+
+/* The CUDA stream (cudaStream_t) every launch of this context is issued on,
+ * so callers can time work with events on the launching stream. */
+void* csm_gpu_stream(csm_ctx* ctx);
+
+/* Waits until every submitted update has a result, or timeout_ns passes
+ * (0 = no limit). */
+int csm_gpu_wait(csm_ctx* ctx, uint64_t timeout_ns);
+
+/* Copies results of updates [first_seq, first_seq + n) to host memory.
+ * Implies csm_gpu_wait for those updates. */
+int csm_gpu_results(csm_ctx* ctx, uint64_t first_seq, uint64_t n, csm_result* out);
+
+/* Device pointer of the result array of the last completed submit (n
+ * entries, in submit order); valid until the next submit. */
+int csm_gpu_results_device(csm_ctx* ctx, const csm_result** d_out, uint64_t* n);
+
+int csm_gpu_stats(csm_ctx* ctx, csm_stats* out);
+
+/* Number of distinct kernel launches issued by this context so far. */
+uint64_t csm_gpu_kernel_launches(csm_ctx* ctx);
+
+void csm_gpu_destroy(csm_ctx* ctx);
+
+/* Text of the last error on this thread. */
+const char* csm_gpu_last_error(void);
+const char* csm_gpu_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSM_GPU_H */

@@ -1,0 +1,813 @@
+// C ABI of the engine: context, device memory, query plans, the per-batch
+// launch sequence, results.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "csm_host.cuh"
+#include "csm_index.cuh"
+#include "csm_kernels.cuh"
+
+namespace csm {
+
+static thread_local std::string g_last_error;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) return set_err(CSM_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,       \
+                                          cudaGetErrorString(e_));                                    \
+  } while (0)
+
+#define CKL()                                                                                         \
+  do {                                                                                                \
+    ctx->launches++;                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                              \
+    if (e_ != cudaSuccess) return set_err(CSM_ECUDA, "%s:%d launch: %s", __FILE__, __LINE__,          \
+                                          cudaGetErrorString(e_));                                    \
+  } while (0)
+
+static uint32_t ceil_log2(uint64_t x) {
+  uint32_t b = 0;
+  while ((1ULL << b) < x) b++;
+  return b;
+}
+
+static inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)std::max<uint64_t>(1, (n + t - 1) / t); }
+
+}  // namespace csm
+
+using namespace csm;
+
+struct csm_ctx {
+  csm_cfg cfg;
+  int dev = 0, sm_count = 0;
+  cudaStream_t st = nullptr;
+  DevMem mem;
+  uint64_t launches = 0;
+  // query
+  bool has_query = false;
+  uint32_t nq = 0;
+  std::vector<uint32_t> qvl, qe;      // labels, (u, v, l) triples (deduplicated)
+  std::vector<std::vector<uint32_t>> qnbr, qel;  // sorted adjacency
+  Plan* h_plan = nullptr;
+  Plan* d_plan = nullptr;
+  size_t plan_bytes = 0;
+  bool has_plan = false;
+  // graph
+  bool has_graph = false;
+  DevGraph g{};
+  uint64_t num_edges = 0;
+  // candidate index
+  IndexState index{};
+  // batch buffers
+  uint32_t bmax = 0, lcap = 0, task_cap = 0;
+  csm_update* d_stream = nullptr; uint64_t stream_cap = 0;
+  uint64_t *d_ukey = nullptr, *d_ukey2 = nullptr;
+  uint32_t *d_useq = nullptr, *d_useq2 = nullptr;
+  UpdInfo* d_info = nullptr;
+  uint64_t *d_ins = nullptr, *d_ins2 = nullptr, *d_del = nullptr, *d_del2 = nullptr;
+  uint64_t *d_tk = nullptr, *d_tk2 = nullptr, *d_ts = nullptr, *d_ts2 = nullptr;
+  VRange *d_rins = nullptr, *d_rdel = nullptr, *d_rt = nullptr;
+  uint32_t* d_ins_dst = nullptr;
+  unsigned int* d_cnt = nullptr;  // [0] n_ins [1] n_del [2] n_t [3] n_rins [4] n_rdel [5] n_rt [6] n_tasks [7] task_next
+  Task* d_tasks = nullptr;
+  unsigned long long *d_count = nullptr, *d_hash = nullptr, *d_bytes = nullptr;
+  unsigned int* d_stop = nullptr;
+  uint32_t* d_safe = nullptr;
+  unsigned long long* d_stamp = nullptr;  // [0] submit time (globaltimer)
+  csm_result* d_results = nullptr; uint64_t results_cap = 0;
+  void* d_cub = nullptr; size_t cub_bytes = 0;
+  // bookkeeping
+  uint64_t seq_next = 0, last_first = 0, last_n = 0;
+  uint64_t updates_done = 0, v_updates = 0, e_updates = 0, batches = 0;
+  uint64_t tot_pos = 0, tot_neg = 0, tot_unsafe = 0;
+  bool totals_dirty = false;
+  std::vector<csm_result> h_last;  // host copy of the last submit's results (filled lazily)
+  bool h_last_valid = false;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+  double last_ms = 0, total_ms = 0;
+  // CUDA events around every search launch of the pending submit
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sev;
+  size_t sev_used = 0;
+  uint64_t search_launches = 0, work_bytes = 0;
+  double search_ms = 0;
+};
+
+namespace csm {
+
+// ------------------------------------------------------------------ plans
+
+// GraphFlow matching orders (ParaCOSM/CSM/matching/GraphFlow/graphflow.cpp:36-169):
+// order 0 starts at the max-degree query vertex; order i > 0 starts at the
+// i-th backward edge of order 0; every next vertex maximises the number of
+// already ordered neighbours, ties broken by larger degree, then smaller id.
+static void graphflow_orders(const csm_ctx* ctx, std::vector<std::vector<uint32_t>>& order) {
+  const uint32_t n = ctx->nq, m = (uint32_t)(ctx->qe.size() / 3);
+  order.assign(m, std::vector<uint32_t>(n, 0));
+  std::vector<uint32_t> offs(n, 0), csr(m + 1, 0);
+  auto deg = [&](uint32_t u) { return (uint32_t)ctx->qnbr[u].size(); };
+  auto pick = [&](std::vector<char>& vis) {
+    uint32_t best = kNone, best_adj = 0;
+    for (uint32_t j = 0; j < n; j++) {
+      if (vis[j]) continue;
+      uint32_t adj = 0;
+      for (uint32_t o : ctx->qnbr[j]) if (vis[o]) adj++;
+      if (!adj) continue;
+      if (best == kNone || (adj == best_adj && deg(j) > deg(best)) || adj > best_adj) { best_adj = adj; best = j; }
+    }
+    return best;
+  };
+  std::vector<char> vis(n, 0);
+  uint32_t maxd = 0;
+  for (uint32_t i = 0; i < n; i++) if (deg(i) > maxd) { maxd = deg(i); order[0][0] = i; }
+  vis[order[0][0]] = 1;
+  for (uint32_t i = 1; i < n; i++) {
+    const uint32_t u = pick(vis);
+    order[0][i] = u; vis[u] = 1;
+    offs[i] = offs[i - 1];
+    for (uint32_t o : ctx->qnbr[u]) if (vis[o]) csr[offs[i]++] = o;
+  }
+  for (uint32_t i = 1; i < m; i++) {
+    std::vector<char> v2(n, 0);
+    const uint32_t p = (uint32_t)(std::lower_bound(offs.begin(), offs.end(), i + 1) - offs.begin());
+    order[i][0] = order[0][p];
+    order[i][1] = csr[i];
+    v2[order[i][0]] = 1; v2[order[i][1]] = 1;
+    for (uint32_t j = 2; j < n; j++) { const uint32_t u = pick(v2); order[i][j] = u; v2[u] = 1; }
+  }
+}
+
+static uint32_t qedge_label(const csm_ctx* ctx, uint32_t a, uint32_t b) {
+  const auto& nb = ctx->qnbr[a];
+  auto it = std::lower_bound(nb.begin(), nb.end(), b);
+  if (it == nb.end() || *it != b) return kNone;
+  return ctx->qel[a][(size_t)(it - nb.begin())];
+}
+
+static int build_plan(csm_ctx* ctx) {
+  std::vector<std::vector<uint32_t>> order;
+  graphflow_orders(ctx, order);
+  Plan* P = ctx->h_plan;
+  memset(P, 0, sizeof(Plan));
+  P->n = ctx->nq;
+  P->n_anchor = (uint32_t)order.size();
+  const uint32_t n_el = ctx->g.n_el;
+  for (uint32_t a = 0; a < P->n_anchor; a++) {
+    PlanAnchor& A = P->anchors[a];
+    const auto& o = order[a];
+    A.la = ctx->qvl[o[0]]; A.lb = ctx->qvl[o[1]]; A.el = qedge_label(ctx, o[0], o[1]);
+    uint32_t nb_total = 0;
+    for (uint32_t d = 0; d < ctx->nq; d++) {
+      PlanPos& pp = A.pos[d];
+      pp.qv = (uint8_t)o[d];
+      pp.nb = 0; pp.boff = (uint16_t)nb_total; pp.samelab = 0;
+      if (d < 2) continue;
+      for (uint32_t j = 0; j < d; j++) {
+        if (ctx->qvl[o[j]] == ctx->qvl[o[d]]) pp.samelab |= 1u << j;
+        const uint32_t l = qedge_label(ctx, o[d], o[j]);
+        if (l == kNone) continue;
+        if (nb_total >= kMaxQE || pp.nb >= kMaxBack) return set_err(CSM_EUNSUPPORTED, "query too dense");
+        A.back_pos[nb_total] = (uint8_t)j;
+        A.back_combo[nb_total] = (uint16_t)(ctx->qvl[o[d]] * n_el + l);
+        nb_total++; pp.nb++;
+      }
+      if (pp.nb == 0) return set_err(CSM_EINVAL, "query graph is not connected");
+    }
+  }
+  ctx->plan_bytes = offsetof(Plan, anchors) + (size_t)P->n_anchor * sizeof(PlanAnchor);
+  if (!ctx->d_plan) {
+    int rc = ctx->mem.alloc((void**)&ctx->d_plan, sizeof(Plan));
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->d_plan, P, ctx->plan_bytes, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->has_plan = true;
+  return CSM_OK;
+}
+
+// --------------------------------------------------------- batch buffers
+
+static int ensure_batch_buffers(csm_ctx* ctx) {
+  if (ctx->d_ukey) return CSM_OK;
+  const uint32_t B = ctx->bmax;
+  const uint32_t L = 4 * B + 64;
+  ctx->lcap = L;
+  const uint32_t na = std::max<uint32_t>(1, (uint32_t)(ctx->qe.size() / 3));
+  ctx->task_cap = B * 2 * na;
+  DevMem& m = ctx->mem;
+  int rc = 0;
+#define AL(p, sz) do { rc = m.alloc((void**)&(p), (sz)); if (rc) return rc; } while (0)
+  AL(ctx->d_ukey, 8ull * B); AL(ctx->d_ukey2, 8ull * B);
+  AL(ctx->d_useq, 4ull * B); AL(ctx->d_useq2, 4ull * B);
+  AL(ctx->d_info, sizeof(UpdInfo) * (size_t)B);
+  AL(ctx->d_ins, 8ull * L); AL(ctx->d_ins2, 8ull * L);
+  AL(ctx->d_del, 8ull * L); AL(ctx->d_del2, 8ull * L);
+  AL(ctx->d_tk, 8ull * L); AL(ctx->d_tk2, 8ull * L);
+  AL(ctx->d_ts, 8ull * L); AL(ctx->d_ts2, 8ull * L);
+  AL(ctx->d_rins, sizeof(VRange) * (size_t)L); AL(ctx->d_rdel, sizeof(VRange) * (size_t)L);
+  AL(ctx->d_rt, sizeof(VRange) * (size_t)L);
+  AL(ctx->d_ins_dst, 4ull * L);
+  AL(ctx->d_cnt, 64);
+  AL(ctx->d_tasks, sizeof(Task) * (size_t)ctx->task_cap);
+  AL(ctx->d_count, 8ull * B); AL(ctx->d_hash, 8ull * B); AL(ctx->d_bytes, 8ull * B);
+  AL(ctx->d_stop, 4ull * B); AL(ctx->d_safe, 4ull * B);
+  AL(ctx->d_stamp, 64);
+#undef AL
+  // CUB scratch: the largest of the sorts issued per batch
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, ctx->d_ukey, ctx->d_ukey2, ctx->d_useq, ctx->d_useq2, (int)B, 0, 64, ctx->st));
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, b2, ctx->d_ins, ctx->d_ins2, (int)L, 0, 64, ctx->st));
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, ctx->d_tk, ctx->d_tk2, ctx->d_ts, ctx->d_ts2, (int)L, 0, 64, ctx->st));
+  const size_t need = std::max(b1, std::max(b2, b3));
+  if (need > ctx->cub_bytes) {
+    if (ctx->d_cub) ctx->mem.release(ctx->d_cub, ctx->cub_bytes);
+    ctx->d_cub = nullptr;
+    rc = ctx->mem.alloc(&ctx->d_cub, need);
+    if (rc) return rc;
+    ctx->cub_bytes = need;
+  }
+  return CSM_OK;
+}
+
+static int ensure_results(csm_ctx* ctx, uint64_t n) {
+  if (n <= ctx->results_cap) return CSM_OK;
+  if (ctx->d_results) ctx->mem.release(ctx->d_results, ctx->results_cap * sizeof(csm_result));
+  ctx->d_results = nullptr;
+  uint64_t cap = std::max<uint64_t>(n, 1024);
+  int rc = ctx->mem.alloc((void**)&ctx->d_results, cap * sizeof(csm_result));
+  if (rc) return rc;
+  ctx->results_cap = cap;
+  return CSM_OK;
+}
+
+static int ensure_stream(csm_ctx* ctx, uint64_t n) {
+  if (n <= ctx->stream_cap) return CSM_OK;
+  if (ctx->d_stream) ctx->mem.release(ctx->d_stream, ctx->stream_cap * sizeof(csm_update));
+  ctx->d_stream = nullptr;
+  uint64_t cap = std::max<uint64_t>(n, 1024);
+  int rc = ctx->mem.alloc((void**)&ctx->d_stream, cap * sizeof(csm_update));
+  if (rc) return rc;
+  ctx->stream_cap = cap;
+  return CSM_OK;
+}
+
+__global__ void k_stamp(unsigned long long* stamp) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  stamp[0] = t;
+}
+
+__global__ void k_latency(uint32_t B, const unsigned long long* stamp, csm_result* out) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= B) return;
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  out[s].latency_ns = t - stamp[0];
+}
+
+// Launch sequence of one batch of B edge updates already in device memory.
+static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_result* out) {
+  cudaStream_t st = ctx->st;
+  DevGraph& g = ctx->g;
+  const uint32_t L = std::min<uint32_t>(ctx->lcap, 4 * B + 64);
+  const KeyBits kb = g.kb;
+  CK(cudaMemsetAsync(ctx->d_cnt, 0, 64, st));
+  CK(cudaMemsetAsync(ctx->d_ins, 0xff, 8ull * L, st));
+  CK(cudaMemsetAsync(ctx->d_del, 0xff, 8ull * L, st));
+  CK(cudaMemsetAsync(ctx->d_tk, 0xff, 8ull * L, st));
+  CK(cudaMemsetAsync(ctx->d_count, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(ctx->d_bytes, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(ctx->d_stop, 0, 4ull * B, st));
+  if (ctx->cfg.want_hash) CK(cudaMemsetAsync(ctx->d_hash, 0, 8ull * B, st));
+  unsigned int* c = ctx->d_cnt;
+
+  k_batch_init<<<blocks_for(B, 256), 256, 0, st>>>(ups, B, g, ctx->d_ukey, ctx->d_useq, ctx->d_info); CKL();
+  size_t tb = ctx->cub_bytes;
+  CK(cub::DeviceRadixSort::SortPairs(ctx->d_cub, tb, ctx->d_ukey, ctx->d_ukey2, ctx->d_useq, ctx->d_useq2, (int)B, 0, 64, st));
+  ResolveOut ro{ctx->d_ins, c + 0, ctx->d_del, c + 1, ctx->d_tk, ctx->d_ts, c + 2, L};
+  k_resolve<<<blocks_for(B, 128), 128, 0, st>>>(ctx->d_ukey2, ctx->d_useq2, B, g, ups, ctx->d_info, ro); CKL();
+  const int end_bit = (int)kb.total();
+  tb = ctx->cub_bytes;
+  CK(cub::DeviceRadixSort::SortKeys(ctx->d_cub, tb, ctx->d_ins, ctx->d_ins2, (int)L, 0, end_bit, st));
+  tb = ctx->cub_bytes;
+  CK(cub::DeviceRadixSort::SortKeys(ctx->d_cub, tb, ctx->d_del, ctx->d_del2, (int)L, 0, end_bit, st));
+  tb = ctx->cub_bytes;
+  CK(cub::DeviceRadixSort::SortPairs(ctx->d_cub, tb, ctx->d_tk, ctx->d_tk2, ctx->d_ts, ctx->d_ts2, (int)L, 0, end_bit, st));
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_ins2, L, kb, ctx->d_rins, c + 3); CKL();
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_del2, L, kb, ctx->d_rdel, c + 4); CKL();
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_tk2, L, kb, ctx->d_rt, c + 5); CKL();
+  g.t_key = ctx->d_tk2;
+  g.t_span = reinterpret_cast<int2*>(ctx->d_ts2);
+  k_temporal_set<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
+  // CSR -> union graph (relocating rows, and compacting the pools first if needed)
+  k_reloc_need<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rins, c + 3, g); CKL();
+  k_compact_check<<<1, 1, 0, st>>>(g); CKL();
+  k_compact_copy<<<ctx->sm_count * 4, 1024, 0, st>>>(g); CKL();
+  k_compact_finish<<<1, 1, 0, st>>>(g); CKL();
+  const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
+  k_mut_insert<<<mut_blocks, 256, 0, st>>>(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g); CKL();
+  // candidate index: union-graph insertions
+  int rc = index_apply_insertions(ctx->index, g, ctx->d_ins2, c + 3, ctx->d_rins, st, &ctx->launches);
+  if (rc) return rc;
+  // search
+  k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, ctx->d_info, g, ctx->d_plan, ctx->index.d2, ctx->index.words,
+                                              ctx->d_tasks, c + 6, ctx->task_cap, ctx->d_safe, &g.ps->error); CKL();
+  SearchParams sp{};
+  sp.g = g; sp.plan = ctx->d_plan; sp.tasks = ctx->d_tasks; sp.n_tasks = c + 6; sp.task_cap = ctx->task_cap;
+  sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash; sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
+  sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = ctx->cfg.max_results;
+  sp.homo = ctx->cfg.homomorphism; sp.want_hash = ctx->cfg.want_hash; sp.error = &g.ps->error;
+  uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
+  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
+  uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
+  if (!bps) {
+    const size_t smem = search_smem_bytes(ctx->nq, warps);
+    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
+  }
+  if (ctx->sev_used == ctx->sev.size()) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    ctx->sev.emplace_back(a, b);
+  }
+  CK(cudaEventRecord(ctx->sev[ctx->sev_used].first, st));
+  launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
+  CK(cudaEventRecord(ctx->sev[ctx->sev_used].second, st));
+  ctx->sev_used++;
+  k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, ctx->d_info, ctx->d_count, ctx->d_hash, ctx->d_bytes,
+                                                  ctx->d_safe, ctx->cfg.max_results, ctx->cfg.want_hash, out); CKL();
+  k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, ctx->d_stamp, out); CKL();
+  // union graph -> CSR after the batch
+  k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, g); CKL();
+  rc = index_apply_deletions(ctx->index, g, ctx->d_del2, c + 4, ctx->d_rdel, st, &ctx->launches);
+  if (rc) return rc;
+  k_temporal_clear<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
+  ctx->batches++;
+  return CSM_OK;
+}
+
+static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_update& h, csm_result* out) {
+  cudaStream_t st = ctx->st;
+  if (h.is_add && h.id1 < ctx->g.n_cap && h.id1 >= ctx->g.n) ctx->g.n = h.id1 + 1;
+  k_vertex_update<<<1, 32, 0, st>>>(ups, 1, ctx->g, ctx->d_info); CKL();
+  CK(cudaMemsetAsync(ctx->d_safe, 0xff, 4, st));
+  k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, 0, 0, out); CKL();
+  int rc = index_vertex_update(ctx->index, ctx->g, ups, st, &ctx->launches);
+  return rc;
+}
+
+static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, const csm_update* h_ups) {
+  if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
+  int rc = ensure_batch_buffers(ctx);
+  if (rc) return rc;
+  rc = ensure_results(ctx, n);
+  if (rc) return rc;
+  cudaStream_t st = ctx->st;
+  CK(cudaEventRecord(ctx->ev_start, st));
+  k_stamp<<<1, 1, 0, st>>>(ctx->d_stamp); CKL();
+  const uint32_t B = (ctx->cfg.mode == CSM_MODE_PLAIN) ? 1u : ctx->bmax;
+  // vertex updates run on their own; runs of edge updates form batches
+  std::vector<csm_update> hv;
+  const csm_update* h = h_ups;
+  if (!h) {
+    hv.resize(n);
+    CK(cudaMemcpyAsync(hv.data(), d_ups, n * sizeof(csm_update), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h = hv.data();
+  }
+  uint64_t i = 0;
+  while (i < n) {
+    if (h[i].type == 'v') {
+      rc = run_vertex_update(ctx, d_ups + i, h[i], ctx->d_results + i);
+      if (rc) return rc;
+      ctx->v_updates++;
+      i++;
+      continue;
+    }
+    uint64_t j = i;
+    while (j < n && j - i < B && h[j].type != 'v') j++;
+    rc = run_edge_batch(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i);
+    if (rc) return rc;
+    ctx->e_updates += j - i;
+    i = j;
+  }
+  CK(cudaEventRecord(ctx->ev_end, st));
+  ctx->last_first = ctx->seq_next;
+  ctx->last_n = n;
+  ctx->seq_next += n;
+  ctx->updates_done += n;
+  ctx->totals_dirty = true;
+  ctx->h_last_valid = false;
+  return CSM_OK;
+}
+
+static int check_device_error(csm_ctx* ctx) {
+  PoolState ps;
+  CK(cudaMemcpy(&ps, ctx->g.ps, sizeof(PoolState), cudaMemcpyDeviceToHost));
+  if (ps.error) {
+    static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow"};
+    return set_err(CSM_EDEVICE, "device error %u (%s)", ps.error, ps.error < 4 ? names[ps.error] : "?");
+  }
+  return CSM_OK;
+}
+
+// Sums the search-kernel event pairs of completed submits.
+static int collect_search_times(csm_ctx* ctx) {
+  for (size_t i = 0; i < ctx->sev_used; i++) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->sev[i].first, ctx->sev[i].second));
+    ctx->search_ms += ms;
+  }
+  ctx->search_launches += ctx->sev_used;
+  ctx->sev_used = 0;
+  return CSM_OK;
+}
+
+static int fetch_last(csm_ctx* ctx) {
+  if (ctx->h_last_valid) return CSM_OK;
+  CK(cudaStreamSynchronize(ctx->st));
+  {
+    int rc0 = collect_search_times(ctx);
+    if (rc0) return rc0;
+  }
+  int rc = check_device_error(ctx);
+  if (rc) return rc;
+  ctx->h_last.resize(ctx->last_n);
+  if (ctx->last_n) {
+    CK(cudaMemcpyAsync(ctx->h_last.data(), ctx->d_results, ctx->last_n * sizeof(csm_result), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  if (ctx->totals_dirty) {
+    for (const csm_result& r : ctx->h_last) {
+      ctx->tot_pos += r.pos; ctx->tot_neg += r.neg;
+      if (r.pos || r.neg) ctx->tot_unsafe++;
+      ctx->work_bytes += r.work_bytes;
+    }
+    ctx->totals_dirty = false;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_end) == cudaSuccess) { ctx->last_ms = ms; ctx->total_ms += ms; }
+  }
+  ctx->h_last_valid = true;
+  return CSM_OK;
+}
+
+}  // namespace csm
+
+// ================================================================== C ABI
+
+extern "C" {
+
+void csm_gpu_default_cfg(csm_cfg* cfg) {
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->algorithm = CSM_ALGO_GRAPHFLOW;
+  cfg->mode = CSM_MODE_BATCHED;
+  cfg->max_batch = kMaxBatch;
+}
+
+const char* csm_gpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* csm_gpu_strerror(int code) {
+  switch (code) {
+    case CSM_OK: return "ok";
+    case CSM_EINVAL: return "invalid argument";
+    case CSM_ENOMEM: return "out of device memory or HBM budget";
+    case CSM_ECUDA: return "CUDA error";
+    case CSM_ESTATE: return "call out of order";
+    case CSM_EUNSUPPORTED: return "unsupported input";
+    case CSM_ETIMEOUT: return "timed out";
+    case CSM_EDEVICE: return "device-side error";
+    default: return "unknown error";
+  }
+}
+
+int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
+  if (!cfg || !out) return set_err(CSM_EINVAL, "null argument");
+  if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
+  if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(CSM_ECUDA, "no CUDA device");
+  if (cfg->device < 0 || cfg->device >= ndev) return set_err(CSM_EINVAL, "bad device %d", cfg->device);
+  CK(cudaSetDevice(cfg->device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, cfg->device));
+  if (prop.major < 10) return set_err(CSM_EUNSUPPORTED, "needs an sm_100 device, found sm_%d%d", prop.major, prop.minor);
+  csm_ctx* ctx = new csm_ctx();
+  ctx->cfg = *cfg;
+  if (!ctx->cfg.max_batch) ctx->cfg.max_batch = kMaxBatch;
+  ctx->bmax = ctx->cfg.mode == CSM_MODE_PLAIN ? 1u : ctx->cfg.max_batch;
+  ctx->dev = cfg->device;
+  ctx->sm_count = prop.multiProcessorCount;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  ctx->mem.budget = cfg->hbm_budget_bytes ? cfg->hbm_budget_bytes : (uint64_t)(0.9 * (double)free_b);
+  if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_end) != cudaSuccess) {
+    delete ctx;
+    return set_err(CSM_ECUDA, "stream/event creation failed");
+  }
+  ctx->h_plan = new Plan();
+  *out = ctx;
+  return CSM_OK;
+}
+
+int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges) {
+  if (!ctx || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
+  if (ctx->has_graph) return set_err(CSM_ESTATE, "set the query before loading the graph");
+  if (n_qv < 2 || n_qv > kMaxQ) return set_err(CSM_EUNSUPPORTED, "query must have 2..%u vertices", kMaxQ);
+  ctx->nq = n_qv;
+  ctx->qvl.assign(q_vlabels, q_vlabels + n_qv);
+  for (uint32_t l : ctx->qvl) if (l == kNone) return set_err(CSM_EINVAL, "query vertex without a label");
+  ctx->qnbr.assign(n_qv, {});
+  ctx->qel.assign(n_qv, {});
+  ctx->qe.clear();
+  for (uint32_t i = 0; i < n_qe; i++) {
+    const uint32_t a = q_edges[3 * i], b = q_edges[3 * i + 1], l = q_edges[3 * i + 2];
+    if (a >= n_qv || b >= n_qv) return set_err(CSM_EINVAL, "query edge endpoint out of range");
+    if (a == b) continue;
+    auto it = std::lower_bound(ctx->qnbr[a].begin(), ctx->qnbr[a].end(), b);
+    if (it != ctx->qnbr[a].end() && *it == b) continue;  // Graph::AddEdge: repeat is a no-op
+    size_t d = (size_t)(it - ctx->qnbr[a].begin());
+    ctx->qnbr[a].insert(it, b); ctx->qel[a].insert(ctx->qel[a].begin() + (long)d, l);
+    it = std::lower_bound(ctx->qnbr[b].begin(), ctx->qnbr[b].end(), a);
+    d = (size_t)(it - ctx->qnbr[b].begin());
+    ctx->qnbr[b].insert(it, a); ctx->qel[b].insert(ctx->qel[b].begin() + (long)d, l);
+    ctx->qe.push_back(a); ctx->qe.push_back(b); ctx->qe.push_back(l);
+  }
+  if (ctx->qe.empty()) return set_err(CSM_EINVAL, "query has no edges");
+  {  // the edge-anchored search needs a connected query
+    std::vector<char> seen(n_qv, 0);
+    std::vector<uint32_t> stack{0};
+    seen[0] = 1;
+    uint32_t reached = 1;
+    while (!stack.empty()) {
+      uint32_t u = stack.back(); stack.pop_back();
+      for (uint32_t w : ctx->qnbr[u]) if (!seen[w]) { seen[w] = 1; reached++; stack.push_back(w); }
+    }
+    if (reached != n_qv) return set_err(CSM_EUNSUPPORTED, "query graph is not connected");
+  }
+  if (ctx->qe.size() / 3 > kMaxQE) return set_err(CSM_EUNSUPPORTED, "query has more than %u edges", kMaxQE);
+  ctx->has_query = true;
+  return CSM_OK;
+}
+
+int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges) {
+  if (!ctx || (n_v && !vlabels) || (n_e && !edges)) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->has_query) return set_err(CSM_ESTATE, "set the query first");
+  if (ctx->has_graph) return set_err(CSM_ESTATE, "graph already loaded");
+  CK(cudaSetDevice(ctx->dev));
+  cudaStream_t st = ctx->st;
+  // label capacities
+  uint32_t max_vl = 0, max_el = 0;
+  for (uint32_t v = 0; v < n_v; v++) if (vlabels[v] != kNone) max_vl = std::max(max_vl, vlabels[v] + 1);
+  for (uint32_t l : ctx->qvl) max_vl = std::max(max_vl, l + 1);
+  for (uint64_t i = 0; i < n_e; i++) max_el = std::max(max_el, edges[3 * i + 2] + 1);
+  for (size_t i = 0; i < ctx->qe.size(); i += 3) max_el = std::max(max_el, ctx->qe[i + 2] + 1);
+  uint32_t n_vl = std::max(std::max(max_vl, ctx->cfg.vlabel_capacity), 1u);
+  uint32_t n_el = std::max(std::max(max_el, ctx->cfg.elabel_capacity), 1u);
+  if (n_el > 64) return set_err(CSM_EUNSUPPORTED, "at most 64 edge labels are supported");
+  const uint64_t nc = (uint64_t)n_vl * n_el;
+  if (nc > 65535) return set_err(CSM_EUNSUPPORTED, "vertex labels x edge labels above 65535");
+  const uint32_t headroom = ctx->cfg.vertex_headroom ? ctx->cfg.vertex_headroom : 1024;
+  const uint64_t n_cap64 = (uint64_t)n_v + headroom;
+  if (n_cap64 > (1ull << 30)) return set_err(CSM_EUNSUPPORTED, "too many vertices");
+  const uint32_t n_cap = (uint32_t)n_cap64;
+  KeyBits kb{ceil_log2((uint64_t)n_cap + 2), std::max<uint32_t>(1, ceil_log2(nc))};
+  if (kb.total() > 64) return set_err(CSM_EUNSUPPORTED, "vertex id and label widths exceed a 64-bit key");
+  DevGraph& g = ctx->g;
+  g.n = n_v; g.n_cap = n_cap; g.n_vl = n_vl; g.n_el = n_el; g.nc = (uint32_t)nc; g.kb = kb;
+  DevMem& m = ctx->mem;
+  int rc = 0;
+#define AL(p, sz) do { rc = m.alloc((void**)&(p), (sz)); if (rc) return rc; } while (0)
+  AL(g.vlabel, 4ull * n_cap);
+  AL(g.row_off, 8ull * n_cap);
+  AL(g.row_cap, 4ull * n_cap);
+  AL(g.dir, 4ull * n_cap * (nc + 1));
+  AL(g.t_start, 4ull * n_cap);
+  AL(g.t_count, 4ull * n_cap);
+  AL(g.ps, sizeof(PoolState));
+  CK(cudaMemsetAsync(g.vlabel, 0xff, 4ull * n_cap, st));
+  CK(cudaMemcpyAsync(g.vlabel, vlabels, 4ull * n_v, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(g.row_off, 0, 8ull * n_cap, st));
+  CK(cudaMemsetAsync(g.row_cap, 0, 4ull * n_cap, st));
+  CK(cudaMemsetAsync(g.dir, 0, 4ull * n_cap * (nc + 1), st));
+  CK(cudaMemsetAsync(g.t_count, 0, 4ull * n_cap, st));
+  CK(cudaMemsetAsync(g.ps, 0, sizeof(PoolState), st));
+  // temporaries
+  uint32_t* d_e = nullptr; uint64_t *ukey = nullptr, *ukey2 = nullptr, *uidx = nullptr, *uidx2 = nullptr;
+  uint64_t *dkey = nullptr, *dkey2 = nullptr, *first = nullptr, *cap64 = nullptr;
+  unsigned long long* d_small = nullptr;
+  const uint64_t M = 2 * n_e;
+  AL(d_e, 12ull * n_e);
+  AL(ukey, 8ull * n_e); AL(ukey2, 8ull * n_e); AL(uidx, 8ull * n_e); AL(uidx2, 8ull * n_e);
+  AL(d_small, 64);
+  CK(cudaMemcpyAsync(d_e, edges, 12ull * n_e, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_small, 0, 64, st));
+  if (n_e) { k_load_edge_keys<<<blocks_for(n_e, 256), 256, 0, st>>>(d_e, n_e, g.vlabel, n_v, ukey, uidx, d_small); CKL(); }
+  void* tmp = nullptr; size_t tb = 0, tb2 = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, ukey, ukey2, uidx, uidx2, (int64_t)n_e, 0, 64, st));
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tb2, dkey, dkey2, (int64_t)M, 0, (int)kb.total(), st));
+  size_t tb3 = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, cap64, g.row_off, (int64_t)n_cap, st));
+  const size_t tbmax = std::max(tb, std::max(tb2, tb3));
+  AL(tmp, tbmax);
+  if (n_e) {
+    tb = tbmax;
+    CK(cub::DeviceRadixSort::SortPairs(tmp, tb, ukey, ukey2, uidx, uidx2, (int64_t)n_e, 0, 64, st));
+  }
+  unsigned long long bad = 0;
+  CK(cudaMemcpyAsync(&bad, d_small, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  m.release(ukey, 8ull * n_e); m.release(uidx, 8ull * n_e);
+  if (bad) { m.release(d_e, 12ull * n_e); m.release(ukey2, 8ull * n_e); m.release(uidx2, 8ull * n_e);
+             m.release(tmp, tbmax); m.release(d_small, 64);
+             return set_err(CSM_EINVAL, "%llu edges touch a vertex id without a label line", bad); }
+  AL(dkey, 8ull * std::max<uint64_t>(M, 1)); AL(dkey2, 8ull * std::max<uint64_t>(M, 1));
+  if (n_e) { k_load_directed<<<blocks_for(n_e, 256), 256, 0, st>>>(ukey2, uidx2, n_e, d_e, g.vlabel, n_el, kb, dkey); CKL(); }
+  m.release(ukey2, 8ull * n_e); m.release(uidx2, 8ull * n_e); m.release(d_e, 12ull * n_e);
+  if (M) {
+    tb = tbmax;
+    CK(cub::DeviceRadixSort::SortKeys(tmp, tb, dkey, dkey2, (int64_t)M, 0, (int)kb.total(), st));
+  }
+  m.release(dkey, 8ull * std::max<uint64_t>(M, 1));
+  AL(first, 8ull * n_cap); AL(cap64, 8ull * n_cap);
+  if (M) { k_load_count<<<blocks_for(M, 256), 256, 0, st>>>(dkey2, M, kb, (uint32_t)nc, g.dir, first, d_small + 1); CKL(); }
+  k_dir_scan<<<blocks_for(n_cap, 256), 256, 0, st>>>(g.dir, n_cap, (uint32_t)nc); CKL();
+  k_load_caps<<<blocks_for(n_cap, 256), 256, 0, st>>>(g.dir, n_cap, (uint32_t)nc, g.row_cap, cap64); CKL();
+  tb = tbmax;
+  CK(cub::DeviceScan::ExclusiveSum(tmp, tb, cap64, g.row_off, (int64_t)n_cap, st));
+  unsigned long long last_off = 0, last_cap = 0, n_valid = 0;
+  CK(cudaMemcpyAsync(&last_off, g.row_off + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&last_cap, cap64 + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&n_valid, d_small + 1, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const uint64_t used = last_off + last_cap;
+  const uint64_t pool_cap = std::max<uint64_t>(2 * used + 16ull * ctx->bmax + (1ull << 20), 1ull << 20);
+  if (pool_cap >= (1ull << 32)) return set_err(CSM_EUNSUPPORTED, "graph too large for 32-bit pool offsets");
+  g.pool_cap = pool_cap;
+  AL(g.pools[0], 4ull * pool_cap);
+  AL(g.pools[1], 4ull * pool_cap);
+  if (M) { k_load_scatter<<<blocks_for(M, 256), 256, 0, st>>>(dkey2, M, kb, first, g.row_off, g.pools[0]); CKL(); }
+  PoolState ps{};
+  ps.top[0] = used;
+  CK(cudaMemcpyAsync(g.ps, &ps, sizeof(ps), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  m.release(dkey2, 8ull * std::max<uint64_t>(M, 1)); m.release(first, 8ull * n_cap); m.release(cap64, 8ull * n_cap);
+  m.release(tmp, tbmax); m.release(d_small, 64);
+#undef AL
+  ctx->num_edges = n_valid / 2;
+  ctx->has_graph = true;
+  return CSM_OK;
+}
+
+int csm_gpu_build_index(csm_ctx* ctx) {
+  if (!ctx) return set_err(CSM_EINVAL, "null context");
+  if (!ctx->has_graph) return set_err(CSM_ESTATE, "load the graph first");
+  CK(cudaSetDevice(ctx->dev));
+  int rc = build_plan(ctx);
+  if (rc) return rc;
+  rc = ensure_batch_buffers(ctx);
+  if (rc) return rc;
+  IndexQuery q{ctx->nq, &ctx->qvl, &ctx->qnbr, &ctx->qel};
+  return index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->st, &ctx->launches);
+}
+
+int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
+  if (!ctx || !count) return set_err(CSM_EINVAL, "null argument");
+  return set_err(CSM_EUNSUPPORTED, "initial matching is not implemented yet");
+}
+
+int csm_gpu_classify(csm_ctx* ctx, uint64_t n, const csm_update* ups, uint8_t* safe_out) {
+  if (!ctx || (n && (!ups || !safe_out))) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->has_plan) return set_err(CSM_ESTATE, "build the index first");
+  if (!n) return CSM_OK;
+  int rc = ensure_stream(ctx, n);
+  if (rc) return rc;
+  uint8_t* d_safe = nullptr;
+  rc = ctx->mem.alloc((void**)&d_safe, n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->d_stream, ups, n * sizeof(csm_update), cudaMemcpyHostToDevice, ctx->st));
+  k_classify<<<blocks_for(n, 256), 256, 0, ctx->st>>>(n, ctx->d_stream, ctx->g, ctx->d_plan, d_safe); CKL();
+  CK(cudaMemcpyAsync(safe_out, d_safe, n, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->mem.release(d_safe, n);
+  return CSM_OK;
+}
+
+int csm_gpu_submit(csm_ctx* ctx, uint64_t n, const csm_update* ups) {
+  if (!ctx || (n && !ups)) return set_err(CSM_EINVAL, "null argument");
+  CK(cudaSetDevice(ctx->dev));
+  if (!n) return CSM_OK;
+  int rc = ensure_stream(ctx, n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->d_stream, ups, n * sizeof(csm_update), cudaMemcpyHostToDevice, ctx->st));
+  return submit_common(ctx, n, ctx->d_stream, ups);
+}
+
+int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups) {
+  if (!ctx || (n && !d_ups)) return set_err(CSM_EINVAL, "null argument");
+  CK(cudaSetDevice(ctx->dev));
+  if (!n) return CSM_OK;
+  return submit_common(ctx, n, d_ups, nullptr);
+}
+
+int csm_gpu_wait(csm_ctx* ctx, uint64_t timeout_ns) {
+  if (!ctx) return set_err(CSM_EINVAL, "null context");
+  if (timeout_ns) {
+    auto t0 = std::chrono::steady_clock::now();
+    while (cudaEventQuery(ctx->ev_end) == cudaErrorNotReady) {
+      if ((uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count() > timeout_ns)
+        return set_err(CSM_ETIMEOUT, "wait timed out");
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  int rc = collect_search_times(ctx);
+  if (rc) return rc;
+  return check_device_error(ctx);
+}
+
+int csm_gpu_results(csm_ctx* ctx, uint64_t first_seq, uint64_t n, csm_result* out) {
+  if (!ctx || (n && !out)) return set_err(CSM_EINVAL, "null argument");
+  if (first_seq < ctx->last_first || first_seq + n > ctx->last_first + ctx->last_n)
+    return set_err(CSM_EINVAL, "results are kept for the last submit only: [%llu, %llu)",
+                   (unsigned long long)ctx->last_first, (unsigned long long)(ctx->last_first + ctx->last_n));
+  int rc = fetch_last(ctx);
+  if (rc) return rc;
+  memcpy(out, ctx->h_last.data() + (first_seq - ctx->last_first), n * sizeof(csm_result));
+  return CSM_OK;
+}
+
+int csm_gpu_results_device(csm_ctx* ctx, const csm_result** d_out, uint64_t* n) {
+  if (!ctx || !d_out || !n) return set_err(CSM_EINVAL, "null argument");
+  *d_out = ctx->d_results;
+  *n = ctx->last_n;
+  return CSM_OK;
+}
+
+int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
+  if (!ctx || !out) return set_err(CSM_EINVAL, "null argument");
+  int rc = fetch_last(ctx);
+  if (rc) return rc;
+  memset(out, 0, sizeof(*out));
+  out->num_vertices = ctx->g.n;
+  out->updates_done = ctx->updates_done;
+  out->vertex_updates = ctx->v_updates;
+  out->edge_updates = ctx->e_updates;
+  out->positive = ctx->tot_pos; out->negative = ctx->tot_neg; out->unsafe_updates = ctx->tot_unsafe;
+  out->batches = ctx->batches;
+  out->kernel_launches = ctx->launches;
+  out->device_bytes = ctx->mem.bytes;
+  out->pool_capacity = ctx->g.pool_cap;
+  out->last_batch_ms = ctx->last_ms;
+  out->total_device_ms = ctx->total_ms;
+  if (ctx->has_graph) {
+    PoolState ps;
+    CK(cudaMemcpy(&ps, ctx->g.ps, sizeof(ps), cudaMemcpyDeviceToHost));
+    out->pool_entries = ps.top[ps.active];
+  }
+  index_stats(ctx->index, &out->index_entries, &out->index_vertices);
+  out->num_edges = ctx->num_edges;
+  out->search_launches = ctx->search_launches;
+  out->search_ms = ctx->search_ms;
+  out->work_bytes = ctx->work_bytes;
+  return CSM_OK;
+}
+
+uint64_t csm_gpu_kernel_launches(csm_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void* csm_gpu_stream(csm_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+
+void csm_gpu_destroy(csm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->dev);
+  cudaStreamSynchronize(ctx->st);
+  index_free(ctx->index, ctx->mem);
+  ctx->mem.free_all();
+  for (auto& e : ctx->sev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_end) cudaEventDestroy(ctx->ev_end);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx->h_plan;
+  delete ctx;
+}
+
+}  // extern "C"

@@ -1,0 +1,444 @@
+// Data-graph kernels: load-time CSR build, per-batch resolution of edge
+// lifetimes, in-place slack-block insertion / deletion, pool compaction.
+//
+// Reference semantics restated here:
+//   Graph::AddEdge  (ParaCOSM/CSM/graph/graph.cpp:58-93)  sorted insert, duplicate = no-op
+//   Graph::RemoveEdge (ParaCOSM/CSM/graph/graph.cpp:95-116) sorted erase, missing edge = error
+//   Graph::GetEdgeLabel (ParaCOSM/CSM/graph/graph.cpp:133-174) label of an existing edge
+#include "csm_kernels.cuh"
+
+namespace csm {
+
+// ---------------------------------------------------------------------
+// load-time CSR build
+// ---------------------------------------------------------------------
+
+__global__ void k_load_edge_keys(const uint32_t* e, uint64_t m, const uint32_t* vlabel, uint32_t n,
+                                 uint64_t* key, uint64_t* idx, unsigned long long* bad) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t a = e[3 * i], b = e[3 * i + 1];
+  idx[i] = i;
+  if (a == b) { key[i] = ~0ULL; return; }  // self loops are dropped
+  if (a >= n || b >= n || vlabel[a] == kNone || vlabel[b] == kNone) {
+    key[i] = ~0ULL;
+    atomicAdd(bad, 1ULL);
+    return;
+  }
+  key[i] = ((uint64_t)min(a, b) << 32) | (uint64_t)max(a, b);
+}
+
+// One directed entry pair per distinct undirected edge; repeats (same
+// endpoints, later in the input) are dropped, so the first label wins.
+__global__ void k_load_directed(const uint64_t* ukey, const uint64_t* uidx, uint64_t m, const uint32_t* e,
+                                const uint32_t* vlabel, uint32_t n_el, KeyBits kb, uint64_t* dkey) {
+  uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint64_t k = ukey[j];
+  if (k == ~0ULL || (j > 0 && ukey[j - 1] == k)) {
+    dkey[2 * j] = kb.sentinel();
+    dkey[2 * j + 1] = kb.sentinel();
+    return;
+  }
+  const uint64_t i = uidx[j];
+  const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k, l = e[3 * i + 2];
+  dkey[2 * j] = kb.pack(x, vlabel[y] * n_el + l, y);
+  dkey[2 * j + 1] = kb.pack(y, vlabel[x] * n_el + l, x);
+}
+
+// Per (vertex, combo) run lengths (into dir, scanned later) and the first
+// position of each vertex in the sorted keys.
+__global__ void k_load_count(const uint64_t* dkey, uint64_t M, KeyBits kb, uint32_t nc, uint32_t* dir,
+                             uint64_t* first, unsigned long long* n_valid) {
+  uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= M) return;
+  const uint64_t k = dkey[j];
+  const uint64_t sent = kb.sentinel();
+  if (k == sent) return;
+  const uint32_t x = kb.x_of(k), c = kb.c_of(k);
+  if ((j + 1 == M) || dkey[j + 1] == sent) *n_valid = j + 1;
+  const bool head_x = (j == 0) || kb.x_of(dkey[j - 1]) != x;
+  if (head_x) first[x] = j;
+  const bool head_c = head_x || kb.c_of(dkey[j - 1]) != c;
+  if (head_c) {
+    uint64_t t = j;  // walk to the end of this (x, c) run
+    while (t + 1 < M && dkey[t + 1] != sent && kb.x_of(dkey[t + 1]) == x && kb.c_of(dkey[t + 1]) == c) t++;
+    dir[(size_t)x * (nc + 1) + c] = (uint32_t)(t - j + 1);
+  }
+}
+
+__device__ __forceinline__ uint32_t slack_cap(uint32_t d) { return d == 0 ? 0u : d + max(2u, d >> 2); }
+__device__ __forceinline__ uint32_t grow_cap(uint32_t d) { return d + max(8u, d >> 1); }
+
+__global__ void k_load_caps(const uint32_t* dir, uint32_t n_cap, uint32_t nc, uint32_t* cap, uint64_t* cap64) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_cap) return;
+  const uint32_t c = slack_cap(dir[(size_t)v * (nc + 1) + nc]);
+  cap[v] = c;
+  cap64[v] = c;
+}
+
+__global__ void k_load_scatter(const uint64_t* dkey, uint64_t M, KeyBits kb, const uint64_t* first,
+                               const uint64_t* row_off, uint32_t* pool) {
+  uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= M) return;
+  const uint64_t k = dkey[j];
+  if (k == kb.sentinel()) return;
+  const uint32_t x = kb.x_of(k);
+  pool[row_off[x] + (j - first[x])] = kb.y_of(k);
+}
+
+// Turns per-combo counts into row-relative segment offsets; dir[nc] = degree.
+__global__ void k_dir_scan(uint32_t* dir, uint32_t n_cap, uint32_t nc) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_cap) return;
+  uint32_t* d = dir + (size_t)v * (nc + 1);
+  uint32_t run = 0;
+  for (uint32_t c = 0; c < nc; c++) { uint32_t t = d[c]; d[c] = run; run += t; }
+  d[nc] = run;
+}
+
+// ---------------------------------------------------------------------
+// batch preparation
+// ---------------------------------------------------------------------
+
+__global__ void k_batch_init(const csm_update* ups, uint32_t B, DevGraph g, uint64_t* ukey, uint32_t* useq,
+                             UpdInfo* info) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= B) return;
+  const csm_update u = ups[s];
+  UpdInfo inf;
+  inf.v1 = u.id1; inf.v2 = u.id2; inf.label = u.label; inf.flags = 0;
+  useq[s] = s;
+  uint64_t key = ~0ULL;
+  if (u.type == 'e') {
+    const bool ok = u.id1 < g.n && u.id2 < g.n && u.id1 != u.id2 && g.vlabel[u.id1] != kNone &&
+                    g.vlabel[u.id2] != kNone && (!u.is_add || u.label < g.n_el);
+    if (ok) {
+      key = ((uint64_t)min(u.id1, u.id2) << 32) | (uint64_t)max(u.id1, u.id2);
+      inf.flags = UF_VALID | (u.is_add ? UF_ADD : 0u);
+    } else {
+      inf.flags = UF_INVALID;
+    }
+  }
+  ukey[s] = key;
+  info[s] = inf;
+}
+
+// Finds edge (x, y) in the union graph; returns its label or kNone.
+__device__ uint32_t find_label(const DevGraph& g, const uint32_t* pool, uint32_t x, uint32_t y) {
+  const uint32_t ly = g.vlabel[y];
+  for (uint32_t l = 0; l < g.n_el; l++) {
+    uint64_t lo, hi;
+    segment(g, x, ly * g.n_el + l, lo, hi);
+    if (contains_u32(pool, lo, hi, y)) return l;
+  }
+  return kNone;
+}
+
+__device__ __forceinline__ void emit2(uint64_t* key, unsigned int* n, uint32_t cap, uint64_t k1, uint64_t k2,
+                                      uint64_t* val, uint64_t v, unsigned int* err) {
+  unsigned int i = atomicAdd(n, 2u);
+  if (i + 2 > cap) { atomicExch(err, kErrListOverflow); return; }
+  key[i] = k1; key[i + 1] = k2;
+  if (val) { val[i] = v; val[i + 1] = v; }
+}
+
+// One thread per distinct edge key of the batch walks that edge's updates in
+// sequence order, starting from its state before the batch.  It decides each
+// update's effect (insert, duplicate insert, delete, delete of a missing
+// edge), the label a deletion counts with, the presence intervals of the
+// edge inside the batch, and the row insertions (before the search) and row
+// deletions (after it) that turn the CSR into the union graph and back.
+__global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B, DevGraph g,
+                          const csm_update* ups, UpdInfo* info, ResolveOut out) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= B) return;
+  const uint64_t k = skey[j];
+  if (k == ~0ULL || (j > 0 && skey[j - 1] == k)) return;
+  const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+  const uint32_t lx = g.vlabel[x], ly = g.vlabel[y];
+  const uint32_t* pool = g.pools[g.ps->active];
+  const uint32_t l0 = find_label(g, pool, x, y);
+  const bool present0 = (l0 != kNone);
+  bool cur_p = present0;
+  uint32_t cur_l = present0 ? l0 : 0u;
+  int32_t cur_s = -1;
+  uint64_t ins_mask = 0;
+  unsigned int* err = &g.ps->error;
+  for (uint32_t e = j; e < B && skey[e] == k; e++) {
+    const uint32_t s = sseq[e];
+    UpdInfo inf = info[s];
+    const uint32_t label = ups[s].label;
+    if (inf.flags & UF_ADD) {
+      if (cur_p) {
+        inf.label = label;  // duplicate insert: graph unchanged, counted with the given label
+      } else {
+        cur_p = true; cur_l = label; cur_s = (int32_t)s;
+        inf.label = label; inf.flags |= UF_MUT;
+        if (!(present0 && label == l0)) ins_mask |= 1ULL << label;
+      }
+    } else {
+      if (!cur_p) {
+        inf.flags |= UF_INVALID;  // deleting a missing edge
+      } else {
+        inf.label = cur_l; inf.flags |= UF_MUT;
+        const uint64_t span = (uint64_t)(uint32_t)cur_s | ((uint64_t)(uint32_t)s << 32);
+        emit2(out.t_key, out.n_t, out.cap, g.kb.pack(x, ly * g.n_el + cur_l, y), g.kb.pack(y, lx * g.n_el + cur_l, x),
+              out.t_span, span, err);
+        cur_p = false;
+      }
+    }
+    info[s] = inf;
+  }
+  if (cur_p && cur_s >= 0) {
+    const uint64_t span = (uint64_t)(uint32_t)cur_s | ((uint64_t)(uint32_t)kTimeInf << 32);
+    emit2(out.t_key, out.n_t, out.cap, g.kb.pack(x, ly * g.n_el + cur_l, y), g.kb.pack(y, lx * g.n_el + cur_l, x),
+          out.t_span, span, err);
+  }
+  for (uint64_t m = ins_mask; m; m &= m - 1) {
+    const uint32_t l = (uint32_t)__ffsll((long long)m) - 1;
+    emit2(out.ins_key, out.n_ins, out.cap, g.kb.pack(x, ly * g.n_el + l, y), g.kb.pack(y, lx * g.n_el + l, x),
+          nullptr, 0, err);
+  }
+  const uint64_t uni = ins_mask | (present0 ? (1ULL << l0) : 0ULL);
+  const uint64_t endm = cur_p ? (1ULL << cur_l) : 0ULL;
+  for (uint64_t m = uni & ~endm; m; m &= m - 1) {
+    const uint32_t l = (uint32_t)__ffsll((long long)m) - 1;
+    emit2(out.del_key, out.n_del, out.cap, g.kb.pack(x, ly * g.n_el + l, y), g.kb.pack(y, lx * g.n_el + l, x),
+          nullptr, 0, err);
+  }
+}
+
+// Appends one VRange per vertex run of a sorted packed-key list.
+__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cap) return;
+  const uint64_t sent = kb.sentinel();
+  const uint64_t k = key[j];
+  if (k == sent) return;
+  const uint32_t x = kb.x_of(k);
+  if (j > 0 && kb.x_of(key[j - 1]) == x) return;
+  uint32_t t = j + 1;
+  while (t < cap && key[t] != sent && kb.x_of(key[t]) == x) t++;
+  unsigned int i = atomicAdd(n_ranges, 1u);
+  ranges[i] = VRange{x, j, t - j, 0};
+}
+
+__global__ void k_temporal_set(const VRange* ranges, const unsigned int* n_ranges, DevGraph g) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *n_ranges) return;
+  const VRange r = ranges[i];
+  g.t_start[r.x] = r.start;
+  g.t_count[r.x] = r.count;
+}
+
+__global__ void k_temporal_clear(const VRange* ranges, const unsigned int* n_ranges, DevGraph g) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *n_ranges) return;
+  g.t_count[ranges[i].x] = 0;
+}
+
+__global__ void k_reloc_need(const VRange* ranges, const unsigned int* n_ranges, DevGraph g) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long need = 0;
+  if (i < *n_ranges) {
+    const VRange r = ranges[i];
+    const uint32_t deg = g.dir[(size_t)r.x * (g.nc + 1) + g.nc];
+    if (deg + r.count > g.row_cap[r.x]) need = grow_cap(deg + r.count);
+  }
+  // warp-aggregated add
+  for (int o = 16; o; o >>= 1) need += __shfl_down_sync(0xffffffffu, need, o);
+  if ((threadIdx.x & 31) == 0 && need) atomicAdd(&g.ps->need, need);
+}
+
+__global__ void k_compact_check(DevGraph g) {
+  PoolState* ps = g.ps;
+  const unsigned long long free_slots = g.pool_cap - ps->top[ps->active];
+  ps->compact = (ps->need > free_slots) ? 1u : 0u;
+}
+
+// Copies every row into the other pool with fresh slack (runs only when the
+// active pool cannot absorb this batch's relocations).
+__global__ void k_compact_copy(DevGraph g) {
+  PoolState* ps = g.ps;
+  if (!ps->compact) return;
+  const uint32_t src = ps->active, dst = 1u - src;
+  const uint32_t* sp = g.pools[src];
+  uint32_t* dp = g.pools[dst];
+  __shared__ unsigned long long base;
+  __shared__ uint32_t scan[1024];
+  for (uint64_t v0 = (uint64_t)blockIdx.x * blockDim.x; v0 < g.n_cap; v0 += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = v0 + threadIdx.x;
+    uint32_t deg = 0, cap = 0;
+    if (v < g.n_cap) { deg = g.dir[v * (g.nc + 1) + g.nc]; cap = slack_cap(deg); }
+    scan[threadIdx.x] = cap;
+    __syncthreads();
+    for (uint32_t o = 1; o < blockDim.x; o <<= 1) {  // inclusive scan
+      uint32_t t = threadIdx.x >= o ? scan[threadIdx.x - o] : 0;
+      __syncthreads();
+      scan[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (threadIdx.x == blockDim.x - 1) base = atomicAdd(&ps->top[dst], (unsigned long long)scan[threadIdx.x]);
+    __syncthreads();
+    if (v < g.n_cap) {
+      const uint64_t off = base + scan[threadIdx.x] - cap;
+      const uint64_t so = g.row_off[v];
+      for (uint32_t i = 0; i < deg; i++) dp[off + i] = sp[so + i];
+      g.row_off[v] = off;
+      g.row_cap[v] = cap;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_compact_finish(DevGraph g) {
+  PoolState* ps = g.ps;
+  if (ps->compact) {
+    ps->top[ps->active] = 0;
+    ps->active = 1u - ps->active;
+    ps->compact = 0;
+  }
+  ps->need = 0;
+}
+
+// Combo of the row-relative entry index i: upper_bound(dir, i) - 1.
+__device__ __forceinline__ uint32_t combo_at(const uint32_t* dirx, uint32_t nc, uint32_t i) {
+  uint32_t lo = 0, hi = nc;  // find last c with dirx[c] <= i
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (dirx[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* a, uint32_t lo, uint32_t hi, uint64_t x) {
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// One warp per vertex: merges the vertex's sorted insert list into its row,
+// in place (moving old entries right, back to front) or into a larger row.
+__global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
+                             uint32_t* ins_dst, DevGraph g) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nr = *n_ranges;
+  PoolState* ps = g.ps;
+  uint32_t* pool = g.pools[ps->active];
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nr; w += (gridDim.x * blockDim.x) >> 5) {
+    const VRange r = ranges[w];
+    const uint32_t x = r.x, s = r.start, k = r.count;
+    uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
+    const uint32_t deg = dirx[g.nc];
+    const uint64_t off = g.row_off[x];
+    const uint32_t new_deg = deg + k;
+    uint64_t dst_off = off;
+    uint32_t new_cap = 0;
+    bool fail = false;
+    if (new_deg > g.row_cap[x]) {
+      new_cap = grow_cap(new_deg);
+      unsigned long long o = 0;
+      if (lane == 0) {
+        o = atomicAdd(&ps->top[ps->active], (unsigned long long)new_cap);
+        if (o + new_cap > g.pool_cap) { atomicExch(&ps->error, kErrPoolFull); o = ~0ULL; }
+      }
+      o = __shfl_sync(0xffffffffu, o, 0);
+      if (o == ~0ULL) fail = true;
+      dst_off = o;
+    }
+    if (fail) continue;
+    // 1. destinations of the inserted entries, from the old row
+    for (uint32_t j = lane; j < k; j += 32) {
+      const uint64_t key = ins_key[s + j];
+      const uint32_t c = g.kb.c_of(key), y = g.kb.y_of(key);
+      const uint64_t p = lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
+      ins_dst[s + j] = (uint32_t)p + j;
+    }
+    __syncwarp();
+    // 2. old entries, back to front
+    for (int64_t base = (int64_t)deg; base > 0; base -= 32) {
+      const int64_t i = base - 1 - lane;
+      uint32_t y = 0, dst = 0;
+      if (i >= 0) {
+        y = pool[off + i];
+        const uint32_t c = combo_at(dirx, g.nc, (uint32_t)i);
+        const uint32_t sh = lower_bound_u64(ins_key, s, s + k, g.kb.pack(x, c, y)) - s;
+        dst = (uint32_t)i + sh;
+      }
+      __syncwarp();
+      if (i >= 0) pool[dst_off + dst] = y;
+      __syncwarp();
+    }
+    // 3. inserted entries
+    for (uint32_t j = lane; j < k; j += 32) pool[dst_off + ins_dst[s + j]] = g.kb.y_of(ins_key[s + j]);
+    __syncwarp();
+    // 4. directory
+    for (uint32_t c = lane; c <= g.nc; c += 32) {
+      const uint32_t add = lower_bound_u64(ins_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;
+      dirx[c] += add;
+    }
+    if (lane == 0 && new_cap) { g.row_off[x] = dst_off; g.row_cap[x] = new_cap; }
+    __syncwarp();
+  }
+}
+
+// One warp per vertex: removes the vertex's sorted delete list from its row
+// in place (front to back).
+__global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
+                             DevGraph g) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nr = *n_ranges;
+  uint32_t* pool = g.pools[g.ps->active];
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nr; w += (gridDim.x * blockDim.x) >> 5) {
+    const VRange r = ranges[w];
+    const uint32_t x = r.x, s = r.start, k = r.count;
+    uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
+    const uint32_t deg = dirx[g.nc];
+    const uint64_t off = g.row_off[x];
+    for (uint32_t base = 0; base < deg; base += 32) {
+      const uint32_t i = base + lane;
+      uint32_t y = 0, dst = 0;
+      bool keep = false;
+      if (i < deg) {
+        y = pool[off + i];
+        const uint32_t c = combo_at(dirx, g.nc, i);
+        const uint64_t key = g.kb.pack(x, c, y);
+        const uint32_t p = lower_bound_u64(del_key, s, s + k, key);
+        keep = !(p < s + k && del_key[p] == key);
+        dst = i - (p - s);
+      }
+      __syncwarp();
+      if (keep) pool[off + dst] = y;
+      __syncwarp();
+    }
+    for (uint32_t c = lane; c <= g.nc; c += 32) {
+      const uint32_t sub = lower_bound_u64(del_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;
+      dirx[c] -= sub;
+    }
+    __syncwarp();
+  }
+}
+
+// Vertex insertion (Graph::AddVertex, ParaCOSM/CSM/graph/graph.cpp:23-49): sets
+// the label of an absent vertex slot.  Vertex deletion is flagged invalid by
+// the caller.
+__global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= B) return;
+  const csm_update u = ups[s];
+  if (u.type != 'v') return;
+  UpdInfo inf;
+  inf.v1 = u.id1; inf.v2 = 0; inf.label = u.label; inf.flags = 0;
+  if (u.is_add && u.id1 < g.n_cap && u.label < g.n_vl) {
+    if (g.vlabel[u.id1] == kNone) g.vlabel[u.id1] = u.label;
+  } else {
+    inf.flags = UF_INVALID;
+  }
+  info[s] = inf;
+}
+
+}  // namespace csm

@@ -1,0 +1,79 @@
+// Kernel entry points of the engine (defined in csm_kernels.cu and
+// csm_search.cu), launched by the context in csm_api.cu.
+#pragma once
+#include "csm_internal.cuh"
+
+namespace csm {
+
+// A run of consecutive entries of one vertex in a sorted packed-key list.
+struct VRange {
+  uint32_t x, start, count, pad;
+};
+
+// ---- load-time CSR build (csm_kernels.cu) ----
+__global__ void k_load_edge_keys(const uint32_t* e, uint64_t m, const uint32_t* vlabel, uint32_t n,
+                                 uint64_t* key, uint64_t* idx, unsigned long long* bad);
+__global__ void k_load_directed(const uint64_t* ukey, const uint64_t* uidx, uint64_t m, const uint32_t* e,
+                                const uint32_t* vlabel, uint32_t n_el, KeyBits kb, uint64_t* dkey);
+__global__ void k_load_count(const uint64_t* dkey, uint64_t M, KeyBits kb, uint32_t nc, uint32_t* dir,
+                             uint64_t* first, unsigned long long* n_valid);
+__global__ void k_load_caps(const uint32_t* dir, uint32_t n_cap, uint32_t nc, uint32_t* cap, uint64_t* cap64);
+__global__ void k_load_scatter(const uint64_t* dkey, uint64_t M, KeyBits kb, const uint64_t* first,
+                               const uint64_t* row_off, uint32_t* pool);
+__global__ void k_dir_scan(uint32_t* dir, uint32_t n_cap, uint32_t nc);
+
+// ---- batch preparation ----
+__global__ void k_batch_init(const csm_update* ups, uint32_t B, DevGraph g, uint64_t* ukey, uint32_t* useq,
+                             UpdInfo* info);
+struct ResolveOut {
+  uint64_t* ins_key; unsigned int* n_ins;
+  uint64_t* del_key; unsigned int* n_del;
+  uint64_t* t_key; uint64_t* t_span; unsigned int* n_t;
+  uint32_t cap;  // capacity of each list
+};
+__global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B, DevGraph g,
+                          const csm_update* ups, UpdInfo* info, ResolveOut out);
+__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges);
+__global__ void k_temporal_set(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
+__global__ void k_temporal_clear(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
+__global__ void k_reloc_need(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
+__global__ void k_compact_check(DevGraph g);
+__global__ void k_compact_copy(DevGraph g);
+__global__ void k_compact_finish(DevGraph g);
+__global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
+                             uint32_t* ins_dst, DevGraph g);
+__global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
+                             DevGraph g);
+__global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
+
+// ---- search (csm_search.cu) ----
+struct SearchParams {
+  DevGraph g;
+  const Plan* plan;
+  const Task* tasks;
+  const unsigned int* n_tasks;
+  uint32_t task_cap;
+  unsigned int* task_next;
+  const UpdInfo* info;
+  unsigned long long* count;   // per update of the batch
+  unsigned long long* hash;    // per update of the batch
+  unsigned long long* bytes;   // per update: algorithmic bytes of the expanded nodes
+  unsigned int* stop;          // per update: cap reached
+  const uint64_t* d2;          // optional candidate filter bitsets [n_q][d2_words]
+  uint64_t d2_words;
+  uint64_t cap;                // 0 = none
+  int homo;
+  int want_hash;
+  unsigned int* error;
+};
+__global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
+                       uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
+                       uint32_t* safe, unsigned int* error);
+size_t search_smem_bytes(uint32_t n_q, uint32_t warps);
+void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);
+__global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
+                           const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
+                           uint64_t cap, int want_hash, csm_result* out);
+__global__ void k_classify(uint64_t n, const csm_update* ups, DevGraph g, const Plan* plan, uint8_t* safe);
+
+}  // namespace csm

@@ -1,0 +1,105 @@
+"""Regenerates the golden fixtures under tests/golden/ from the reference itself.
+
+Each case is a small seeded workload (written by paracosm_b200/_bin/csm_gen)
+run through the reference plugins compiled from their sources
+(oracle/_ref/ref_driver, built by `make -C oracle/ref_build`) with the
+sequential per-update semantics of the reference's SingleThreadUpdate loop.
+The fixture keeps the inputs in the reference's text formats and, per
+update, the positive / negative counts of each plugin and the match-set hash
+of sequential SymBi (parsed from its --print-enum output).
+
+    python tests/golden/make_golden.py          # needs the reference sources to build the driver
+
+Only this script reads the reference; the fixtures it writes are plain files.
+"""
+from __future__ import annotations
+
+import json
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from oracle import pyoracle  # noqa: E402
+from paracosm_b200 import workload  # noqa: E402
+
+GEN = ROOT / "paracosm_b200" / "_bin" / "csm_gen"
+
+# name: (generator args, max_results, homo)
+CASES = {
+    "c1_small": (["--preset", "c1", "--log2-n", "11", "--updates", "300", "--seed", "11"], None, False),
+    "mixed_2el": (["--preset", "c2", "--log2-n", "11", "--avg-degree", "6", "--vlabels", "3", "--zipf", "1.0",
+                   "--elabels", "2", "--updates", "400", "--insert-frac", "0.7", "--seed", "12",
+                   "--query", "6:sparse:1"], None, False),
+    "dense_del": (["--preset", "c2", "--log2-n", "10", "--avg-degree", "10", "--vlabels", "3", "--zipf", "0",
+                   "--elabels", "2", "--updates", "300", "--insert-frac", "0.6", "--seed", "13",
+                   "--query", "4:dense"], None, False),
+    "capped": (["--preset", "c2", "--log2-n", "11", "--avg-degree", "8", "--vlabels", "2", "--zipf", "0",
+                "--elabels", "1", "--updates", "200", "--insert-frac", "0.8", "--seed", "14",
+                "--query", "5:sparse:1"], 40, False),
+    "homo": (["--preset", "c2", "--log2-n", "10", "--avg-degree", "8", "--vlabels", "2", "--zipf", "0",
+              "--elabels", "1", "--updates", "200", "--insert-frac", "0.7", "--seed", "15",
+              "--query", "4:sparse:1"], None, True),
+    "zipf_8q": (["--preset", "c2", "--log2-n", "12", "--avg-degree", "8", "--vlabels", "6", "--zipf", "1.2",
+                 "--elabels", "2", "--updates", "300", "--insert-frac", "0.85", "--seed", "16",
+                 "--query", "8:dense"], None, False),
+}
+
+PLUGINS = [("graphflow", 1), ("symbi", 1), ("turboflux", 1), ("parallel_graphflow", 4), ("parallel_turboflux", 4),
+           ("parallel_symbi", 32)]
+
+
+def main() -> None:
+    for name, (args, cap, homo) in CASES.items():
+        d = HERE / name
+        tmp = HERE / f"_tmp_{name}"
+        if tmp.exists():
+            shutil.rmtree(tmp)
+        subprocess.run([str(GEN)] + args + ["--out", str(tmp), "--text"], check=True, capture_output=True)
+        d.mkdir(exist_ok=True)
+        shutil.copy(tmp / "data.graph", d / "data.graph")
+        shutil.copy(tmp / "stream.txt", d / "stream.txt")
+        shutil.copy(tmp / "query_0.graph", d / "query.graph")
+        shutil.rmtree(tmp)
+        cols = {}
+        for algo, threads in PLUGINS:
+            want_hash = algo in ("symbi", "turboflux")
+            kw = {"threads": threads, "want_hash": want_hash}
+            if cap is not None:
+                kw["max_results"] = cap
+            try:
+                rows, _ = pyoracle.ref_run(d / "query.graph", d / "data.graph", d / "stream.txt", algo, timeout=600,
+                                           homo=homo, **kw)
+            except Exception as exc:  # a reference defect (e.g. exit on a deletion) is recorded, not fatal
+                print(f"{name}/{algo}: {exc}".splitlines()[0])
+                continue
+            cols[algo] = rows
+        n = len(workload.read_stream(d / "stream.txt"))
+        with open(d / "expected.csv", "w") as f:
+            hdr = ["idx"]
+            for algo, _ in PLUGINS:
+                if algo in cols:
+                    hdr += [f"{algo}_pos", f"{algo}_neg"]
+                    if algo in ("symbi", "turboflux"):
+                        hdr += [f"{algo}_hash"]
+            f.write(",".join(hdr) + "\n")
+            for i in range(n):
+                row = [str(i)]
+                for algo, _ in PLUGINS:
+                    if algo in cols:
+                        r = cols[algo][i] if i < len(cols[algo]) else None
+                        row += [str(r["pos"]) if r is not None else "", str(r["neg"]) if r is not None else ""]
+                        if algo in ("symbi", "turboflux"):
+                            row += [str(r["hash"]) if r is not None else ""]
+                f.write(",".join(row) + "\n")
+        (d / "params.json").write_text(json.dumps({"max_results": cap, "homo": homo, "generator": args,
+                                                   "plugins": [a for a, _ in PLUGINS if a in cols]}, indent=1))
+        print(name, "updates", n, "plugins", list(cols))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,133 @@
+"""GPU parity: the engine's per-update counts and match-set hashes, through the
+C ABI, against the reference's own outputs (golden fixtures) and the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle import pyoracle
+from paracosm_b200 import ST_CAPPED, ST_INVALID, ST_OK, UPDATE_DTYPE, Engine, workload
+
+pytestmark = pytest.mark.gpu
+
+ALGOS = ["parallel_graphflow", "parallel_turboflux", "parallel_symbi"]
+
+
+def run_engine(qv, qe, vl, e, stream, algo="parallel_graphflow", **kw):
+    kw.setdefault("want_hash", True)
+    with Engine(algo, **kw) as eng:
+        eng.set_query(qv, qe)
+        eng.load_graph(vl, e)
+        eng.build_index()
+        res = eng.run(stream)
+        stats = eng.stats()
+    return res, stats
+
+
+def assert_same(res, pos, neg, hsh=None, cap=0):
+    assert np.array_equal(res["pos"], pos), np.nonzero(res["pos"] != pos)[0][:10]
+    assert np.array_equal(res["neg"], neg), np.nonzero(res["neg"] != neg)[0][:10]
+    if cap:
+        capped = (pos + neg) >= cap
+        assert np.array_equal(res["status"] == ST_CAPPED, capped)
+    if hsh is not None:
+        ok = res["status"] == ST_OK
+        assert np.array_equal(res["hash"][ok], hsh[ok])
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("case", golden_cases())
+def test_golden_batched(case, algo):
+    g = load_golden(case)
+    cap = g["params"]["max_results"] or 0
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], algo, max_results=cap,
+                        homo=g["params"]["homo"])
+    x = g["exp"]
+    assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"], cap)
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_golden_plain_one_update_per_launch(case):
+    g = load_golden(case)
+    cap = g["params"]["max_results"] or 0
+    res, stats = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], max_results=cap, mode="plain",
+                            homo=g["params"]["homo"])
+    x = g["exp"]
+    assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"], cap)
+    assert stats["batches"] == np.sum(g["stream"]["type"] == ord("e"))
+
+
+@pytest.mark.parametrize("max_batch", [2, 7, 64, 333])
+def test_batch_boundaries_do_not_change_results(max_batch):
+    g = load_golden("mixed_2el")
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], max_batch=max_batch)
+    x = g["exp"]
+    assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"])
+
+
+def test_config1_against_oracle(gen_dir):
+    w = workload.generate("c1", gen_dir / "c1")
+    qv, qe = w.queries[0]
+    ref = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream)
+    res, _ = run_engine(qv, qe, w.vlabels, w.edges, w.stream)
+    assert_same(res, ref["pos"], ref["neg"], ref["hash"])
+    assert np.array_equal(res["safe"], ref["safe"])
+
+
+def test_capped_sample_against_oracle(gen_dir):
+    w = workload.generate("c2", gen_dir / "c2cap", extra=["--log2-n", "15", "--updates", "1500"])
+    qv, qe = w.queries[0]
+    cap = 5000
+    ref = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream, max_results=cap)
+    for algo in ALGOS:
+        res, _ = run_engine(qv, qe, w.vlabels, w.edges, w.stream, algo, max_results=cap)
+        assert_same(res, ref["pos"], ref["neg"], ref["hash"], cap)
+
+
+def _toggle_stream():
+    # a small dense graph where one edge is inserted, deleted, re-inserted with
+    # another label, duplicated and deleted again inside one batch
+    n = 8
+    vl = np.zeros(n, dtype=np.uint32)
+    edges = np.array([(a, b, 0) for a in range(n) for b in range(a + 1, n) if (a + b) % 3 != 0], dtype=np.uint32)
+    qv = np.zeros(4, dtype=np.uint32)
+    qe = np.array([(0, 1, 0), (1, 2, 0), (2, 3, 0), (3, 0, 0), (0, 2, 0)], dtype=np.uint32)
+    e = lambda add, a, b, l: (ord("e"), add, 0, a, b, l)  # noqa: E731
+    ups = [e(1, 0, 3, 0), e(0, 0, 3, 0), e(1, 3, 0, 1), e(1, 0, 3, 0), e(0, 3, 0, 1), e(0, 0, 3, 0),
+           e(1, 0, 3, 0), e(0, 1, 2, 0), e(1, 1, 2, 0), e(0, 5, 6, 0), e(0, 5, 6, 0), e(1, 2, 4, 1),
+           e(0, 2, 4, 0), e(1, 0, 6, 0), e(0, 0, 6, 0), e(1, 0, 6, 0)]
+    return vl, edges, qv, qe, np.array(ups, dtype=UPDATE_DTYPE)
+
+
+@pytest.mark.parametrize("max_batch", [1, 3, 65536])
+def test_same_edge_touched_many_times_in_one_batch(max_batch):
+    vl, edges, qv, qe, ups = _toggle_stream()
+    ref = pyoracle.run(qv, qe, vl, edges, ups)
+    res, _ = run_engine(qv, qe, vl, edges, ups, max_batch=max_batch)
+    assert_same(res, ref["pos"], ref["neg"], ref["hash"])
+    assert np.array_equal(res["status"] == ST_INVALID, ref["status"] == pyoracle.ST_INVALID)
+
+
+def test_insert_then_delete_gives_equal_positive_and_negative(gen_dir):
+    w = workload.generate("c1", gen_dir / "c1sym", extra=["--log2-n", "12", "--updates", "400"])
+    qv, qe = w.queries[0]
+    ins = w.stream
+    dels = ins[::-1].copy()
+    dels["is_add"] = 0
+    res, _ = run_engine(qv, qe, w.vlabels, w.edges, np.concatenate([ins, dels]))
+    assert np.array_equal(res["pos"][: len(ins)], res["neg"][len(ins):][::-1])
+    assert np.array_equal(res["hash"][: len(ins)], res["hash"][len(ins):][::-1])
+
+
+def test_vertex_insertion_then_edges():
+    vl = np.array([0, 1, 0, 1], dtype=np.uint32)
+    edges = np.array([(0, 1, 0), (1, 2, 0), (2, 3, 0)], dtype=np.uint32)
+    qv = np.array([0, 1, 0], dtype=np.uint32)
+    qe = np.array([(0, 1, 0), (1, 2, 0)], dtype=np.uint32)
+    ups = np.array([(ord("v"), 1, 0, 4, 0, 0), (ord("e"), 1, 0, 4, 1, 0), (ord("e"), 1, 0, 4, 3, 0)],
+                   dtype=UPDATE_DTYPE)
+    ref = pyoracle.run(qv, qe, vl, edges, ups)
+    res, _ = run_engine(qv, qe, vl, edges, ups)
+    assert_same(res, ref["pos"], ref["neg"], ref["hash"])
+    assert res["pos"][1] > 0
