@@ -136,38 +136,47 @@ def get_workload(cfg: dict, n_updates: int):
     return w
 
 
-def ref_sample(w, algo: str, threads: int, cap: int, budget_s: float, hard_timeout: float, skip: int = 0):
+def ref_sample(w, algo: str, threads: int, cap: int, budget_s: float, hard_timeout: float):
     """Times the reference (oracle/_ref, built from the reference sources) on a bounded
-    prefix of the stream: per-update latencies of the plugin calls."""
+    prefix of the stream.  The driver's watchdog ends the run after `budget_s` seconds
+    of incremental matching even inside an update (parallel TurboFlux ignores the
+    result cap below depth 2), so value = updates completed / incremental seconds."""
     drv = ROOT / "oracle" / "_ref" / "ref_driver"
     if not drv.exists():
         return None, "reference driver not built (oracle/_ref/ref_driver)"
     out = Path(tempfile.mkdtemp()) / "ref.csv"
     cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(w.directory / "data.bin"), "-U",
-           str(w.directory / "stream.bin"), "-a", algo, "-t", str(threads), "--time-budget", str(budget_s),
+           str(w.directory / "stream.bin"), "-a", algo, "-t", str(threads), "--wall-budget", str(budget_s),
            "--out", str(out)]
     if cap:
         cmd += ["--max-results", str(cap)]
     t0 = time.perf_counter()
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=hard_timeout)
-        note = "" if r.returncode == 0 else f"exit {r.returncode}"
     except subprocess.TimeoutExpired:
-        note = f"killed after {hard_timeout:.0f}s (an update ran past the sample budget)"
+        return None, f"reference driver did not finish within {hard_timeout:.0f}s"
     wall = time.perf_counter() - t0
-    if not out.exists():
-        return None, f"no output ({note})"
+    done, elapsed, note = None, None, ""
+    for line in r.stdout.splitlines():
+        if "updates_done=" in line:
+            kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
+            done, elapsed = int(kv["updates_done"]), float(kv["elapsed_s"])
+            if line.startswith("wall_budget_reached"):
+                note = "(budget reached inside an update)"
+    if done is None:
+        return None, f"reference driver failed (exit {r.returncode}): {r.stderr[-300:]}"
     lat = []
-    for line in out.read_text().splitlines()[1:]:
-        parts = line.split(",")
-        if len(parts) >= 10:
-            lat.append(int(parts[8]))
-    lat = np.array(lat[skip:], dtype=np.float64)
-    if len(lat) == 0:
-        return None, f"no update finished ({note})"
-    return {"updates": int(len(lat)), "seconds": float(lat.sum() / 1e9),
-            "value": float(len(lat) / (lat.sum() / 1e9)), "p50_ns": float(np.percentile(lat, 50)),
-            "p99_ns": float(np.percentile(lat, 99)), "wall_s": wall, "note": note}, None
+    if out.exists():
+        for line in out.read_text().splitlines()[1:]:
+            parts = line.split(",")
+            if len(parts) >= 10:
+                lat.append(int(parts[8]))
+    lat = np.array(lat, dtype=np.float64)
+    if done == 0 or elapsed <= 0:
+        return None, f"no update finished within {budget_s:.0f}s {note}".strip()
+    return {"updates": int(done), "seconds": elapsed, "value": done / elapsed,
+            "p50_ns": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ns": float(np.percentile(lat, 99)) if len(lat) else None, "wall_s": wall, "note": note}, None
 
 
 def run_reference_arm(args, cfg):
@@ -179,8 +188,7 @@ def run_reference_arm(args, cfg):
     w = get_workload(cfg, n_updates)
     threads = os.cpu_count() or 1
     budget = float(os.environ.get("CSM_REF_BUDGET_S", "60"))
-    res, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], budget, budget + 600,
-                          skip=args.warmup * steps_upd)
+    res, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], budget, budget + 900)
     line = {"impl": "reference", "metric": METRIC, "unit": "updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "dtype": "u32", "data": "synthetic", "config": {"workload": cfg["workload"]}}
@@ -188,11 +196,11 @@ def run_reference_arm(args, cfg):
         line.update({"value": None, "unavailable": err})
     else:
         line.update({"value": res["value"], "ms_per_step": 1000.0 * steps_upd / res["value"],
-                     "p50_us": res["p50_ns"] / 1e3, "p99_us": res["p99_ns"] / 1e3,
+                     "p50_us": (res["p50_ns"] or 0) / 1e3, "p99_us": (res["p99_ns"] or 0) / 1e3,
                      "cpu_baseline": {"value": res["value"], "unit": "updates/s", "cores": threads,
                                       "kind": "reference",
-                                      "sample": f"first {res['updates']} timed updates of the stream after "
-                                                f"{args.warmup * steps_upd} warm-up updates, "
+                                      "sample": f"first {res['updates']} updates of the stream in "
+                                                f"{res['seconds']:.1f}s of incremental matching, "
                                                 f"parallel_turboflux -t {threads}, {budget:.0f}s budget "
                                                 f"{res['note']}".strip()},
                      "e2e": {"value": res["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
@@ -310,7 +318,7 @@ def main():
     # ---- plain form (one update per launch sequence) on a sample, same initial graph ----
     plain = None
     if rank == 0 and args.plain_sample > 0:
-        P = min(args.plain_sample, W * B)
+        P = min(args.plain_sample, len(stream))
         peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev)
         peng.set_query(qv, qe)
         peng.load_graph(w.vlabels, w.edges)
@@ -339,13 +347,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         r, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], args.cpu_budget,
-                            args.cpu_budget + 400)
+                            args.cpu_budget + 900)
         if r is not None:
             cpu = {"value": r["value"], "unit": "updates/s", "cores": threads, "kind": "reference",
                    "sample": f"first {r['updates']} updates of the same stream, parallel_turboflux -t {threads} "
                              f"(reference sources, sequential update order), {args.cpu_budget:.0f}s budget "
                              f"{r['note']}".strip(),
-                   "p50_us": r["p50_ns"] / 1e3, "p99_us": r["p99_ns"] / 1e3}
+                   "p50_us": (r["p50_ns"] or 0) / 1e3, "p99_us": (r["p99_ns"] or 0) / 1e3}
         else:
             cpu = {"value": None, "unit": "updates/s", "cores": threads, "kind": "reference", "sample": err}
 

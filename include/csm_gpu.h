@@ -8,6 +8,12 @@
  * wraps these entry points in `matching`-style plugin classes so that the
  * csm command line and its output lines are unchanged.
  *
+ * Labels are arbitrary uint32 values.  Internally every vertex label and
+ * edge label that the query does not use is folded into one "inert" label:
+ * such vertices and edges can never be part of an embedding, but they stay
+ * in the graph, so duplicate inserts and deletions behave as in the
+ * reference.
+ *
  * Conventions
  *   - Every int-returning call returns CSM_OK (0) or a negative CSM_E* code;
  *     nothing calls exit() (the reference exits on bad input,
@@ -72,10 +78,8 @@ typedef struct csm_cfg {
                                  (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:975) */
   uint32_t warps_per_block;   /* search kernel tuning; 0 = autotuned */
   uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
-  uint32_t vlabel_capacity;   /* vertex labels the graph may hold; 0 = max seen at load + 1 */
-  uint32_t elabel_capacity;   /* edge labels the graph may hold; 0 = max seen at load + 1 */
   uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */
-  uint32_t reserved[5];
+  uint32_t reserved[7];
 } csm_cfg;
 
 /* Same 16-byte layout as the reference's InsertUnit fields

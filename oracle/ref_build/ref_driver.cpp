@@ -35,6 +35,7 @@
 #include <sstream>
 #include <streambuf>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "graph/graph.h"
@@ -102,9 +103,13 @@ struct Args {
   std::string q, d, u, algo = "graphflow", out, dbin, ubin;
   size_t threads = 1, auto_tuning = 0, max_updates = SIZE_MAX;
   uint64_t max_results = UINT32_MAX;
-  double time_budget = 0;
+  double time_budget = 0;   // stop after the update that crosses this many seconds
+  double wall_budget = 0;   // hard limit: report and exit even inside an update
   bool homo = false, hash = false;
 };
+
+// Completed-update counter shared with the wall-budget watchdog.
+std::atomic<size_t> g_done{0};
 
 bool read_binary_graph(const std::string& path, Graph& g) {
   FILE* f = fopen(path.c_str(), "rb");
@@ -153,7 +158,7 @@ void usage() {
   fprintf(stderr,
           "ref_driver -q query -d data|-D data.bin -u stream|-U stream.bin -a algo\n"
           "  [-t threads] [--auto-tuning 0|1] [--max-results N] [--homo 0|1]\n"
-          "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S]\n");
+          "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S] [--wall-budget S]\n");
 }
 
 }  // namespace
@@ -177,6 +182,7 @@ int main(int argc, char** argv) {
     else if (k == "--out") a.out = nxt();
     else if (k == "--max-updates") a.max_updates = std::stoull(nxt());
     else if (k == "--time-budget") a.time_budget = std::stod(nxt());
+    else if (k == "--wall-budget") a.wall_budget = std::stod(nxt());
     else { usage(); return 2; }
   }
   if (a.q.empty() || (a.d.empty() && a.dbin.empty()) || (a.u.empty() && a.ubin.empty())) { usage(); return 2; }
@@ -221,6 +227,17 @@ int main(int argc, char** argv) {
   size_t pos_last = 0, neg_last = 0, unsafe = 0, nv = 0, ne = 0, done = 0;
   std::vector<uint64_t> lat(n_up, 0);
   auto ts = std::chrono::steady_clock::now();
+  if (a.wall_budget > 0) {
+    // Some reference plugins ignore the result cap inside their parallel
+    // search, so one update can run for hours: report what finished and exit.
+    std::thread([ts, &a]() {
+      std::this_thread::sleep_for(std::chrono::duration<double>(a.wall_budget));
+      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+      printf("wall_budget_reached updates_done=%zu elapsed_s=%.6f\n", g_done.load(), el);
+      fflush(stdout);
+      _exit(0);
+    }).detach();
+  }
   for (size_t i = 0; i < n_up; i++) {
     const InsertUnit& up = data.updates_vec_[i];
     auto s = std::chrono::steady_clock::now();
@@ -237,9 +254,11 @@ int main(int argc, char** argv) {
     if (fo) fprintf(fo, "%zu,%c,%d,%u,%u,%u,%zu,%zu,%llu,%llu\n", i, up.type, (int)up.is_add, up.id1,
                     up.id2, up.label, pc - pos_last, nc - neg_last, (unsigned long long)lat[i],
                     (unsigned long long)h);
+    if (fo) fflush(fo);  // completed updates survive a kill of a run that hangs on a later one
     if (pc != pos_last || nc != neg_last) unsafe++;
     pos_last = pc; neg_last = nc;
     done++;
+    g_done.store(done);
     if (a.time_budget > 0 &&
         std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count() > a.time_budget)
       break;
@@ -261,7 +280,7 @@ int main(int argc, char** argv) {
   printf("Incremental Matching: %.3f ms\n", inc_s * 1e3);
   printf("%zu vertex updates.\n%zu edge updates.\n%zu unsafe updates.\n", nv, ne, unsafe);
   printf("%zu positive matches.\n%zu negative matches.\n", pos_last, neg_last);
-  printf("updates_done=%zu updates_per_s=%.3f p50_ns=%llu p99_ns=%llu threads=%zu\n", done,
+  printf("updates_done=%zu elapsed_s=%.6f updates_per_s=%.3f p50_ns=%llu p99_ns=%llu threads=%zu\n", done, inc_s,
          done / std::max(inc_s, 1e-12), pct(0.50), pct(0.99), a.threads);
   fflush(stdout);
   // Skip destructors of the large hash maps: exit directly.

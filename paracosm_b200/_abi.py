@@ -60,10 +60,8 @@ class CsmCfg(C.Structure):
         ("turboflux_compat", C.c_int32),
         ("warps_per_block", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
-        ("vlabel_capacity", C.c_uint32),
-        ("elabel_capacity", C.c_uint32),
         ("vertex_headroom", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 

@@ -65,7 +65,10 @@ struct csm_ctx {
   // query
   bool has_query = false;
   uint32_t nq = 0;
-  std::vector<uint32_t> qvl, qe;      // labels, (u, v, l) triples (deduplicated)
+  std::vector<uint32_t> qvl, qe;      // labels, (u, v, l) triples (deduplicated), as given
+  std::vector<uint32_t> qlab_v, qlab_e;  // sorted distinct query labels (the label folding tables)
+  std::vector<uint32_t> qvl_f;        // folded query vertex labels
+  uint32_t* d_qlab = nullptr;
   std::vector<std::vector<uint32_t>> qnbr, qel;  // sorted adjacency
   Plan* h_plan = nullptr;
   Plan* d_plan = nullptr;
@@ -93,6 +96,10 @@ struct csm_ctx {
   unsigned int* d_stop = nullptr;
   uint32_t* d_safe = nullptr;
   unsigned long long* d_stamp = nullptr;  // [0] submit time (globaltimer)
+  SearchQueue* d_q = nullptr;
+  DTask* d_dq = nullptr;
+  unsigned int* d_ready = nullptr;
+  uint32_t qcap = 0, epoch = 0;
   csm_result* d_results = nullptr; uint64_t results_cap = 0;
   void* d_cub = nullptr; size_t cub_bytes = 0;
   // bookkeeping
@@ -155,11 +162,17 @@ static void graphflow_orders(const csm_ctx* ctx, std::vector<std::vector<uint32_
   }
 }
 
+static uint32_t fold_host(const std::vector<uint32_t>& sorted, uint32_t l) {
+  auto it = std::lower_bound(sorted.begin(), sorted.end(), l);
+  return (it != sorted.end() && *it == l) ? (uint32_t)(it - sorted.begin()) : (uint32_t)sorted.size();
+}
+
+// Folded label of query edge (a, b), or kNone if a and b are not adjacent.
 static uint32_t qedge_label(const csm_ctx* ctx, uint32_t a, uint32_t b) {
   const auto& nb = ctx->qnbr[a];
   auto it = std::lower_bound(nb.begin(), nb.end(), b);
   if (it == nb.end() || *it != b) return kNone;
-  return ctx->qel[a][(size_t)(it - nb.begin())];
+  return fold_host(ctx->qlab_e, ctx->qel[a][(size_t)(it - nb.begin())]);
 }
 
 static int build_plan(csm_ctx* ctx) {
@@ -173,7 +186,7 @@ static int build_plan(csm_ctx* ctx) {
   for (uint32_t a = 0; a < P->n_anchor; a++) {
     PlanAnchor& A = P->anchors[a];
     const auto& o = order[a];
-    A.la = ctx->qvl[o[0]]; A.lb = ctx->qvl[o[1]]; A.el = qedge_label(ctx, o[0], o[1]);
+    A.la = ctx->qvl_f[o[0]]; A.lb = ctx->qvl_f[o[1]]; A.el = qedge_label(ctx, o[0], o[1]);
     uint32_t nb_total = 0;
     for (uint32_t d = 0; d < ctx->nq; d++) {
       PlanPos& pp = A.pos[d];
@@ -181,12 +194,12 @@ static int build_plan(csm_ctx* ctx) {
       pp.nb = 0; pp.boff = (uint16_t)nb_total; pp.samelab = 0;
       if (d < 2) continue;
       for (uint32_t j = 0; j < d; j++) {
-        if (ctx->qvl[o[j]] == ctx->qvl[o[d]]) pp.samelab |= 1u << j;
+        if (ctx->qvl_f[o[j]] == ctx->qvl_f[o[d]]) pp.samelab |= 1u << j;
         const uint32_t l = qedge_label(ctx, o[d], o[j]);
         if (l == kNone) continue;
         if (nb_total >= kMaxQE || pp.nb >= kMaxBack) return set_err(CSM_EUNSUPPORTED, "query too dense");
         A.back_pos[nb_total] = (uint8_t)j;
-        A.back_combo[nb_total] = (uint16_t)(ctx->qvl[o[d]] * n_el + l);
+        A.back_combo[nb_total] = (uint16_t)(ctx->qvl_f[o[d]] * n_el + l);
         nb_total++; pp.nb++;
       }
       if (pp.nb == 0) return set_err(CSM_EINVAL, "query graph is not connected");
@@ -230,6 +243,12 @@ static int ensure_batch_buffers(csm_ctx* ctx) {
   AL(ctx->d_count, 8ull * B); AL(ctx->d_hash, 8ull * B); AL(ctx->d_bytes, 8ull * B);
   AL(ctx->d_stop, 4ull * B); AL(ctx->d_safe, 4ull * B);
   AL(ctx->d_stamp, 64);
+  ctx->qcap = 1u << 20;
+  AL(ctx->d_q, sizeof(SearchQueue));
+  AL(ctx->d_dq, sizeof(DTask) * (size_t)ctx->qcap);
+  AL(ctx->d_ready, 4ull * ctx->qcap);
+  CK(cudaMemsetAsync(ctx->d_q, 0, sizeof(SearchQueue), ctx->st));
+  CK(cudaMemsetAsync(ctx->d_ready, 0, 4ull * ctx->qcap, ctx->st));
 #undef AL
   // CUB scratch: the largest of the sorts issued per batch
   size_t b1 = 0, b2 = 0, b3 = 0;
@@ -335,6 +354,9 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash; sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
   sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = ctx->cfg.max_results;
   sp.homo = ctx->cfg.homomorphism; sp.want_hash = ctx->cfg.want_hash; sp.error = &g.ps->error;
+  sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.ready = ctx->d_ready; sp.qcap = ctx->qcap; sp.epoch = ++ctx->epoch;
+  sp.wait_limit_ns = 600ull * 1000000000ull;
+  sp.batch = B;
   uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
@@ -423,8 +445,9 @@ static int check_device_error(csm_ctx* ctx) {
   PoolState ps;
   CK(cudaMemcpy(&ps, ctx->g.ps, sizeof(PoolState), cudaMemcpyDeviceToHost));
   if (ps.error) {
-    static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow"};
-    return set_err(CSM_EDEVICE, "device error %u (%s)", ps.error, ps.error < 4 ? names[ps.error] : "?");
+    static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow",
+                                  "search queue wait limit", "malformed donated task"};
+    return set_err(CSM_EDEVICE, "device error %u (%s)", ps.error, ps.error < 6 ? names[ps.error] : "?");
   }
   return CSM_OK;
 }
@@ -553,6 +576,16 @@ int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, ui
     ctx->qe.push_back(a); ctx->qe.push_back(b); ctx->qe.push_back(l);
   }
   if (ctx->qe.empty()) return set_err(CSM_EINVAL, "query has no edges");
+  ctx->qlab_v = ctx->qvl;
+  std::sort(ctx->qlab_v.begin(), ctx->qlab_v.end());
+  ctx->qlab_v.erase(std::unique(ctx->qlab_v.begin(), ctx->qlab_v.end()), ctx->qlab_v.end());
+  ctx->qlab_e.clear();
+  for (size_t i = 0; i < ctx->qe.size(); i += 3) ctx->qlab_e.push_back(ctx->qe[i + 2]);
+  std::sort(ctx->qlab_e.begin(), ctx->qlab_e.end());
+  ctx->qlab_e.erase(std::unique(ctx->qlab_e.begin(), ctx->qlab_e.end()), ctx->qlab_e.end());
+  if (ctx->qlab_e.size() + 1 > 64) return set_err(CSM_EUNSUPPORTED, "at most 63 distinct query edge labels");
+  ctx->qvl_f.resize(n_qv);
+  for (uint32_t u = 0; u < n_qv; u++) ctx->qvl_f[u] = fold_host(ctx->qlab_v, ctx->qvl[u]);
   {  // the edge-anchored search needs a connected query
     std::vector<char> seen(n_qv, 0);
     std::vector<uint32_t> stack{0};
@@ -575,17 +608,10 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
   if (ctx->has_graph) return set_err(CSM_ESTATE, "graph already loaded");
   CK(cudaSetDevice(ctx->dev));
   cudaStream_t st = ctx->st;
-  // label capacities
-  uint32_t max_vl = 0, max_el = 0;
-  for (uint32_t v = 0; v < n_v; v++) if (vlabels[v] != kNone) max_vl = std::max(max_vl, vlabels[v] + 1);
-  for (uint32_t l : ctx->qvl) max_vl = std::max(max_vl, l + 1);
-  for (uint64_t i = 0; i < n_e; i++) max_el = std::max(max_el, edges[3 * i + 2] + 1);
-  for (size_t i = 0; i < ctx->qe.size(); i += 3) max_el = std::max(max_el, ctx->qe[i + 2] + 1);
-  uint32_t n_vl = std::max(std::max(max_vl, ctx->cfg.vlabel_capacity), 1u);
-  uint32_t n_el = std::max(std::max(max_el, ctx->cfg.elabel_capacity), 1u);
-  if (n_el > 64) return set_err(CSM_EUNSUPPORTED, "at most 64 edge labels are supported");
+  // folded label spaces: the query's distinct labels plus one inert label each
+  const uint32_t n_vl = (uint32_t)ctx->qlab_v.size() + 1;
+  const uint32_t n_el = (uint32_t)ctx->qlab_e.size() + 1;
   const uint64_t nc = (uint64_t)n_vl * n_el;
-  if (nc > 65535) return set_err(CSM_EUNSUPPORTED, "vertex labels x edge labels above 65535");
   const uint32_t headroom = ctx->cfg.vertex_headroom ? ctx->cfg.vertex_headroom : 1024;
   const uint64_t n_cap64 = (uint64_t)n_v + headroom;
   if (n_cap64 > (1ull << 30)) return set_err(CSM_EUNSUPPORTED, "too many vertices");
@@ -604,8 +630,17 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
   AL(g.t_start, 4ull * n_cap);
   AL(g.t_count, 4ull * n_cap);
   AL(g.ps, sizeof(PoolState));
+  AL(ctx->d_qlab, 4ull * (ctx->qlab_v.size() + ctx->qlab_e.size()));
+  CK(cudaMemcpyAsync(ctx->d_qlab, ctx->qlab_v.data(), 4ull * ctx->qlab_v.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_qlab + ctx->qlab_v.size(), ctx->qlab_e.data(), 4ull * ctx->qlab_e.size(),
+                     cudaMemcpyHostToDevice, st));
+  g.qlab_v = ctx->d_qlab;
+  g.qlab_e = ctx->d_qlab + ctx->qlab_v.size();
+  g.n_qv = (uint32_t)ctx->qlab_v.size();
+  g.n_qe = (uint32_t)ctx->qlab_e.size();
   CK(cudaMemsetAsync(g.vlabel, 0xff, 4ull * n_cap, st));
   CK(cudaMemcpyAsync(g.vlabel, vlabels, 4ull * n_v, cudaMemcpyHostToDevice, st));
+  if (n_v) { k_fold_vlabels<<<blocks_for(n_v, 256), 256, 0, st>>>(g.vlabel, n_v, g); CKL(); }
   CK(cudaMemsetAsync(g.row_off, 0, 8ull * n_cap, st));
   CK(cudaMemsetAsync(g.row_cap, 0, 4ull * n_cap, st));
   CK(cudaMemsetAsync(g.dir, 0, 4ull * n_cap * (nc + 1), st));
@@ -641,7 +676,7 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
              m.release(tmp, tbmax); m.release(d_small, 64);
              return set_err(CSM_EINVAL, "%llu edges touch a vertex id without a label line", bad); }
   AL(dkey, 8ull * std::max<uint64_t>(M, 1)); AL(dkey2, 8ull * std::max<uint64_t>(M, 1));
-  if (n_e) { k_load_directed<<<blocks_for(n_e, 256), 256, 0, st>>>(ukey2, uidx2, n_e, d_e, g.vlabel, n_el, kb, dkey); CKL(); }
+  if (n_e) { k_load_directed<<<blocks_for(n_e, 256), 256, 0, st>>>(ukey2, uidx2, n_e, d_e, g, dkey); CKL(); }
   m.release(ukey2, 8ull * n_e); m.release(uidx2, 8ull * n_e); m.release(d_e, 12ull * n_e);
   if (M) {
     tb = tbmax;
@@ -686,7 +721,7 @@ int csm_gpu_build_index(csm_ctx* ctx) {
   if (rc) return rc;
   rc = ensure_batch_buffers(ctx);
   if (rc) return rc;
-  IndexQuery q{ctx->nq, &ctx->qvl, &ctx->qnbr, &ctx->qel};
+  IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &ctx->qel};
   return index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->st, &ctx->launches);
 }
 
@@ -786,6 +821,11 @@ int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
   }
   index_stats(ctx->index, &out->index_entries, &out->index_vertices);
   out->num_edges = ctx->num_edges;
+  if (ctx->d_q) {
+    SearchQueue q;
+    CK(cudaMemcpy(&q, ctx->d_q, sizeof(q), cudaMemcpyDeviceToHost));
+    out->donated_tasks = q.donated + std::min<uint64_t>(q.tail, ctx->qcap);
+  }
   out->search_launches = ctx->search_launches;
   out->search_ms = ctx->search_ms;
   out->work_bytes = ctx->work_bytes;

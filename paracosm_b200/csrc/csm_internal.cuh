@@ -56,6 +56,9 @@ struct KeyBits {
   __host__ __device__ uint32_t y_of(uint64_t k) const { return (uint32_t)(k & ((1ULL << yb) - 1)); }
   __host__ __device__ uint32_t total() const { return 2 * yb + cb; }
   __host__ __device__ uint64_t sentinel() const { return total() >= 64 ? ~0ULL : ((1ULL << total()) - 1); }
+  // Real entries are below the sentinel; unused list slots hold the
+  // sentinel or all ones (memset 0xff), both of which fail this test.
+  __host__ __device__ bool real(uint64_t k) const { return k < sentinel(); }
 };
 
 // Bump allocators and flags of the two alternating row pools.
@@ -67,7 +70,8 @@ struct PoolState {
   uint32_t error;             // nonzero: internal error code (see kErr*)
   uint32_t pad;
 };
-enum : uint32_t { kErrNone = 0, kErrPoolFull = 1, kErrListOverflow = 2, kErrTaskOverflow = 3 };
+enum : uint32_t { kErrNone = 0, kErrPoolFull = 1, kErrListOverflow = 2, kErrTaskOverflow = 3, kErrWaitTimeout = 4,
+                  kErrBadTask = 5 };
 
 // Device view of the dynamic CSR (pointers into device memory).
 struct DevGraph {
@@ -83,9 +87,27 @@ struct DevGraph {
   uint64_t* t_key;       // packed keys
   int2* t_span;          // presence interval [start, end] in batch sequence numbers
   uint64_t pool_cap;     // entries per pool
-  uint32_t n, n_cap, n_vl, n_el, nc;
+  // label folding: sorted distinct query labels; label i of the list maps
+  // to i, every other label to the inert label (n_qv / n_qe)
+  const uint32_t* qlab_v;
+  const uint32_t* qlab_e;
+  uint32_t n_qv, n_qe;
+  uint32_t n, n_cap, n_vl, n_el, nc;  // n_vl = n_qv + 1, n_el = n_qe + 1
   KeyBits kb;
 };
+
+__device__ __forceinline__ uint32_t fold_label(const uint32_t* sorted, uint32_t n, uint32_t l) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (sorted[mid] < l) lo = mid + 1; else hi = mid;
+  }
+  return (lo < n && sorted[lo] == l) ? lo : n;
+}
+__device__ __forceinline__ uint32_t fold_vlabel(const DevGraph& g, uint32_t l) {
+  return l == kNone ? kNone : fold_label(g.qlab_v, g.n_qv, l);
+}
+__device__ __forceinline__ uint32_t fold_elabel(const DevGraph& g, uint32_t l) { return fold_label(g.qlab_e, g.n_qe, l); }
 
 __device__ __forceinline__ uint32_t combo_of(const DevGraph& g, uint32_t vl, uint32_t el) {
   return vl * g.n_el + el;

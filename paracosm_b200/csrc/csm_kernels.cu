@@ -28,10 +28,20 @@ __global__ void k_load_edge_keys(const uint32_t* e, uint64_t m, const uint32_t* 
   key[i] = ((uint64_t)min(a, b) << 32) | (uint64_t)max(a, b);
 }
 
+// Folds raw vertex labels to the engine's compact labels (see DevGraph).
+__global__ void k_fold_vlabels(uint32_t* vlabel, uint32_t n, DevGraph g) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  vlabel[v] = fold_vlabel(g, vlabel[v]);
+}
+
 // One directed entry pair per distinct undirected edge; repeats (same
 // endpoints, later in the input) are dropped, so the first label wins.
 __global__ void k_load_directed(const uint64_t* ukey, const uint64_t* uidx, uint64_t m, const uint32_t* e,
-                                const uint32_t* vlabel, uint32_t n_el, KeyBits kb, uint64_t* dkey) {
+                                DevGraph g, uint64_t* dkey) {
+  const KeyBits kb = g.kb;
+  const uint32_t* vlabel = g.vlabel;
+  const uint32_t n_el = g.n_el;
   uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= m) return;
   const uint64_t k = ukey[j];
@@ -41,7 +51,7 @@ __global__ void k_load_directed(const uint64_t* ukey, const uint64_t* uidx, uint
     return;
   }
   const uint64_t i = uidx[j];
-  const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k, l = e[3 * i + 2];
+  const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k, l = fold_elabel(g, e[3 * i + 2]);
   dkey[2 * j] = kb.pack(x, vlabel[y] * n_el + l, y);
   dkey[2 * j + 1] = kb.pack(y, vlabel[x] * n_el + l, x);
 }
@@ -53,16 +63,15 @@ __global__ void k_load_count(const uint64_t* dkey, uint64_t M, KeyBits kb, uint3
   uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= M) return;
   const uint64_t k = dkey[j];
-  const uint64_t sent = kb.sentinel();
-  if (k == sent) return;
+  if (!kb.real(k)) return;
   const uint32_t x = kb.x_of(k), c = kb.c_of(k);
-  if ((j + 1 == M) || dkey[j + 1] == sent) *n_valid = j + 1;
+  if ((j + 1 == M) || !kb.real(dkey[j + 1])) *n_valid = j + 1;
   const bool head_x = (j == 0) || kb.x_of(dkey[j - 1]) != x;
   if (head_x) first[x] = j;
   const bool head_c = head_x || kb.c_of(dkey[j - 1]) != c;
   if (head_c) {
     uint64_t t = j;  // walk to the end of this (x, c) run
-    while (t + 1 < M && dkey[t + 1] != sent && kb.x_of(dkey[t + 1]) == x && kb.c_of(dkey[t + 1]) == c) t++;
+    while (t + 1 < M && kb.real(dkey[t + 1]) && kb.x_of(dkey[t + 1]) == x && kb.c_of(dkey[t + 1]) == c) t++;
     dir[(size_t)x * (nc + 1) + c] = (uint32_t)(t - j + 1);
   }
 }
@@ -83,7 +92,7 @@ __global__ void k_load_scatter(const uint64_t* dkey, uint64_t M, KeyBits kb, con
   uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= M) return;
   const uint64_t k = dkey[j];
-  if (k == kb.sentinel()) return;
+  if (!kb.real(k)) return;
   const uint32_t x = kb.x_of(k);
   pool[row_off[x] + (j - first[x])] = kb.y_of(k);
 }
@@ -108,12 +117,12 @@ __global__ void k_batch_init(const csm_update* ups, uint32_t B, DevGraph g, uint
   if (s >= B) return;
   const csm_update u = ups[s];
   UpdInfo inf;
-  inf.v1 = u.id1; inf.v2 = u.id2; inf.label = u.label; inf.flags = 0;
+  inf.v1 = u.id1; inf.v2 = u.id2; inf.label = fold_elabel(g, u.label); inf.flags = 0;
   useq[s] = s;
   uint64_t key = ~0ULL;
   if (u.type == 'e') {
     const bool ok = u.id1 < g.n && u.id2 < g.n && u.id1 != u.id2 && g.vlabel[u.id1] != kNone &&
-                    g.vlabel[u.id2] != kNone && (!u.is_add || u.label < g.n_el);
+                    g.vlabel[u.id2] != kNone;
     if (ok) {
       key = ((uint64_t)min(u.id1, u.id2) << 32) | (uint64_t)max(u.id1, u.id2);
       inf.flags = UF_VALID | (u.is_add ? UF_ADD : 0u);
@@ -169,7 +178,7 @@ __global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B
   for (uint32_t e = j; e < B && skey[e] == k; e++) {
     const uint32_t s = sseq[e];
     UpdInfo inf = info[s];
-    const uint32_t label = ups[s].label;
+    const uint32_t label = inf.label;  // folded in k_batch_init
     if (inf.flags & UF_ADD) {
       if (cur_p) {
         inf.label = label;  // duplicate insert: graph unchanged, counted with the given label
@@ -214,13 +223,12 @@ __global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B
 __global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= cap) return;
-  const uint64_t sent = kb.sentinel();
   const uint64_t k = key[j];
-  if (k == sent) return;
+  if (!kb.real(k)) return;
   const uint32_t x = kb.x_of(k);
   if (j > 0 && kb.x_of(key[j - 1]) == x) return;
   uint32_t t = j + 1;
-  while (t < cap && key[t] != sent && kb.x_of(key[t]) == x) t++;
+  while (t < cap && kb.real(key[t]) && kb.x_of(key[t]) == x) t++;
   unsigned int i = atomicAdd(n_ranges, 1u);
   ranges[i] = VRange{x, j, t - j, 0};
 }
@@ -284,10 +292,14 @@ __global__ void k_compact_copy(DevGraph g) {
     __syncthreads();
     if (v < g.n_cap) {
       const uint64_t off = base + scan[threadIdx.x] - cap;
-      const uint64_t so = g.row_off[v];
-      for (uint32_t i = 0; i < deg; i++) dp[off + i] = sp[so + i];
-      g.row_off[v] = off;
-      g.row_cap[v] = cap;
+      if (off + cap > g.pool_cap) {
+        atomicExch(&ps->error, kErrPoolFull);
+      } else {
+        const uint64_t so = g.row_off[v];
+        for (uint32_t i = 0; i < deg; i++) dp[off + i] = sp[so + i];
+        g.row_off[v] = off;
+        g.row_cap[v] = cap;
+      }
     }
     __syncthreads();
   }
@@ -433,8 +445,8 @@ __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, U
   if (u.type != 'v') return;
   UpdInfo inf;
   inf.v1 = u.id1; inf.v2 = 0; inf.label = u.label; inf.flags = 0;
-  if (u.is_add && u.id1 < g.n_cap && u.label < g.n_vl) {
-    if (g.vlabel[u.id1] == kNone) g.vlabel[u.id1] = u.label;
+  if (u.is_add && u.id1 < g.n_cap) {
+    if (g.vlabel[u.id1] == kNone) g.vlabel[u.id1] = fold_vlabel(g, u.label);
   } else {
     inf.flags = UF_INVALID;
   }

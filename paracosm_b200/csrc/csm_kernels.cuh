@@ -13,8 +13,9 @@ struct VRange {
 // ---- load-time CSR build (csm_kernels.cu) ----
 __global__ void k_load_edge_keys(const uint32_t* e, uint64_t m, const uint32_t* vlabel, uint32_t n,
                                  uint64_t* key, uint64_t* idx, unsigned long long* bad);
+__global__ void k_fold_vlabels(uint32_t* vlabel, uint32_t n, DevGraph g);
 __global__ void k_load_directed(const uint64_t* ukey, const uint64_t* uidx, uint64_t m, const uint32_t* e,
-                                const uint32_t* vlabel, uint32_t n_el, KeyBits kb, uint64_t* dkey);
+                                DevGraph g, uint64_t* dkey);
 __global__ void k_load_count(const uint64_t* dkey, uint64_t M, KeyBits kb, uint32_t nc, uint32_t* dir,
                              uint64_t* first, unsigned long long* n_valid);
 __global__ void k_load_caps(const uint32_t* dir, uint32_t n_cap, uint32_t nc, uint32_t* cap, uint64_t* cap64);
@@ -47,6 +48,26 @@ __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges,
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
 
 // ---- search (csm_search.cu) ----
+// Donated search task: a partial match of positions 0..depth (depth 1 = the
+// updated edge itself) and the driver range of position depth + 1.
+struct DTask {
+  uint32_t upd;
+  uint16_t anchor;
+  uint8_t orient;
+  uint8_t depth;
+  uint32_t dlo, dn, dsel;
+  uint32_t m[kMaxQ];
+  uint32_t pad[3];
+};
+static_assert(sizeof(DTask) == 160, "DTask is 160 bytes");
+
+// Work queue of one search launch.  `pending` counts tasks (root and
+// donated) not finished yet; idle warps exit when it reaches zero.
+struct SearchQueue {
+  unsigned int head, tail, idle, pending;
+  unsigned long long donated;  // tasks handed over by earlier launches
+};
+
 struct SearchParams {
   DevGraph g;
   const Plan* plan;
@@ -65,6 +86,14 @@ struct SearchParams {
   int homo;
   int want_hash;
   unsigned int* error;
+  // work donation (null dq: off)
+  SearchQueue* q;
+  DTask* dq;
+  unsigned int* ready;        // ready[i] == epoch once dq[i] is filled
+  uint32_t qcap;
+  uint32_t epoch;
+  unsigned long long wait_limit_ns;
+  uint32_t batch;             // updates in this batch (bound of task update indices)
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,

@@ -133,6 +133,290 @@ __device__ __forceinline__ bool pick_driver(const SearchParams& p, const PlanAnc
   return !empty;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Per-task accumulators, flushed to the update's counters when the task ends.
+struct TaskAcc {
+  unsigned long long cnt, hash, bytes;
+};
+
+// Hands unexpanded work at the shallowest level with work left to idle warps:
+// whole entries from the end of that level's buffer, or, when only the entry
+// in progress is left, the upper half of its remaining driver range.  Each
+// donated task is a partial match (positions 0..L) plus a driver range for
+// position L + 1.  Returns the number of tasks handed over.
+__device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t lane, uint32_t idle_now,
+                           uint32_t t, const Task& T, uint32_t m0, uint32_t m1) {
+  int Ls = 0;
+  uint32_t mode = 0;  // 1: whole entries, 2: split the entry in progress
+  for (int L = 1; L <= d; L++) {
+    const uint32_t cnt = lv[L].cnt, ce = lv[L].cur_e;
+    if (ce >= cnt) continue;
+    if (cnt - ce >= 2) { Ls = L; mode = 1; break; }
+    if (lv[L].dn[ce] - lv[L].cur_k >= 64) { Ls = L; mode = 2; break; }
+  }
+  if (!mode) return 0;
+  LevelSM& S = lv[Ls];
+  const uint32_t cnt = S.cnt, ce = S.cur_e;
+  uint32_t k = mode == 1 ? min(min(idle_now, cnt - ce - 1), 32u) : 1u;
+  unsigned int base = 0;
+  if (lane == 0) {
+    base = atomicAdd(&p.q->tail, k);
+    const unsigned int ok = base >= p.qcap ? 0u : min(k, p.qcap - base);
+    if (ok) atomicAdd(&p.q->pending, ok);
+    k = ok;
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  k = __shfl_sync(0xffffffffu, k, 0);
+  if (k == 0) return 0;
+  // entry handed to lane j and its driver range
+  uint32_t e = 0, dlo = 0, dn = 0;
+  if (mode == 1) {
+    e = cnt - k + lane;
+    if (lane < k) { dlo = S.dlo[e]; dn = S.dn[e]; }
+  } else {
+    e = ce;
+    const uint32_t rem = S.dn[ce] - S.cur_k, keep = rem >> 1;
+    dlo = S.dlo[ce] + S.cur_k + keep;
+    dn = rem - keep;
+  }
+  if (lane < k) {
+    DTask* D = p.dq + base + lane;
+    uint32_t idx = e;
+    for (int L = Ls; L >= 2; --L) { D->m[L] = lv[L].v[idx]; idx = lv[L].par[idx]; }
+    D->m[0] = m0; D->m[1] = m1;
+    D->upd = t; D->anchor = T.anchor; D->orient = T.orient; D->depth = (uint8_t)Ls;
+    D->dlo = dlo; D->dn = dn; D->dsel = S.dsel[e];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    if (mode == 1) S.cnt = cnt - k;
+    else S.dn[ce] = S.cur_k + ((S.dn[ce] - S.cur_k) >> 1);
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane < k) *(volatile unsigned int*)(p.ready + base + lane) = p.epoch;
+  __syncwarp();
+  return k;
+}
+
+// Depth-first walk over chunked levels starting at level `d` (see the file
+// comment); positions 0 and 1 hold m0 and m1.
+__device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int d, uint32_t lane,
+                           const Task& T, const PlanAnchor* A, uint32_t m0, uint32_t m1, TaskAcc& acc) {
+  const uint32_t n = p.plan->n;
+  const uint32_t t = T.upd;
+  volatile unsigned int* stop = p.stop;
+  uint32_t iter = 0;
+  while (d >= 1) {
+    ++iter;
+    if ((iter & 7) == 0) {
+      uint32_t st = (lane == 0) ? stop[t] : 0u;
+      if (__shfl_sync(0xffffffffu, st, 0)) break;
+    }
+    if ((iter & 15) == 0 && p.dq) {
+      uint32_t idle_now = (lane == 0) ? *(volatile unsigned int*)&p.q->idle : 0u;
+      idle_now = __shfl_sync(0xffffffffu, idle_now, 0);
+      if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1);
+    }
+    LevelSM& L = lv[d];
+    const uint32_t cnt = L.cnt, ce = L.cur_e, ck = L.cur_k;
+    if (ce >= cnt) { d--; continue; }
+    // the next 32 (entry, driver element) pairs of this level
+    const uint32_t el = ce + lane;
+    const uint32_t rem = (el < cnt) ? L.dn[el] - (lane == 0 ? ck : 0u) : 0u;
+    const uint32_t incl = warp_incl_scan(rem, lane);
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t owner = 0;
+#pragma unroll
+    for (uint32_t step = 16; step; step >>= 1) {
+      const uint32_t v = __shfl_sync(0xffffffffu, incl, owner + step - 1);
+      if (v <= lane) owner += step;
+    }
+    const uint32_t prev = __shfl_sync(0xffffffffu, incl, owner > 0 ? (owner - 1) & 31 : 0);
+    const bool active = lane < total;
+    const uint32_t e = ce + owner;
+    const uint32_t kk = lane - (owner > 0 ? prev : 0u) + (owner == 0 ? ck : 0u);
+    uint32_t nce, nck;
+    if (total <= 32) {
+      nce = ce + min(32u, cnt - ce); nck = 0;
+    } else {
+      const uint32_t o31 = __shfl_sync(0xffffffffu, owner, 31);
+      const uint32_t k31 = __shfl_sync(0xffffffffu, kk, 31);
+      const uint32_t e31 = ce + o31;
+      if (k31 + 1 >= L.dn[e31]) { nce = e31 + 1; nck = 0; } else { nce = e31; nck = k31 + 1; }
+    }
+    const uint32_t pos = (uint32_t)d + 1;
+    bool valid = false;
+    uint32_t x = 0, ndlo = 0, ndn = 0, ndsel = 0;
+    unsigned long long nb4 = 0;
+    uint32_t m[kMaxQ];
+    if (active) {
+      x = pool[(uint64_t)L.dlo[e] + kk];
+      m[0] = m0; m[1] = m1;
+      uint32_t idx = e;
+      for (int l2 = d; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
+      valid = check_candidate(p, pool, A, pos, x, m, L.dsel[e], (int32_t)t);
+      if (valid && pos + 1 < n) {
+        m[pos] = x;
+        valid = pick_driver(p, A, pos + 1, m, (int32_t)t, ndlo, ndn, ndsel, nb4);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) { L.cur_e = nce; L.cur_k = nck; }
+    const uint32_t mask = __ballot_sync(0xffffffffu, valid);
+    if (pos + 1 < n) {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) nb4 += __shfl_xor_sync(0xffffffffu, nb4, o);
+      acc.bytes += nb4;
+    }
+    if (pos == n - 1) {
+      const uint32_t c = __popc(mask);
+      if (p.want_hash) {
+        unsigned long long h = 0;
+        if (valid) {
+          uint64_t s = pair_hash(A->pos[pos].qv, x);
+          for (uint32_t q = 0; q < pos; q++) s += pair_hash(A->pos[q].qv, m[q]);
+          h = mix64(s);
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+        acc.hash += h;
+      }
+      acc.cnt += c;
+      if (c && p.cap) {
+        unsigned int hit = 0;
+        if (lane == 0) {
+          const unsigned long long old = atomicAdd(&p.count[t], acc.cnt);
+          acc.cnt = 0;
+          if (old + c >= p.cap) { stop[t] = 1u; hit = 1; }
+        }
+        if (__shfl_sync(0xffffffffu, hit, 0)) break;
+      }
+    } else {
+      LevelSM& N = lv[pos];
+      if (valid) {
+        const uint32_t slot = __popc(mask & ((1u << lane) - 1u));
+        N.v[slot] = x; N.par[slot] = (uint8_t)e; N.dlo[slot] = ndlo; N.dn[slot] = ndn;
+        N.dsel[slot] = (uint8_t)ndsel;
+      }
+      if (lane == 0) { N.cnt = __popc(mask); N.cur_e = 0; N.cur_k = 0; }
+      __syncwarp();
+      if (mask) d = (int)pos;
+    }
+  }
+}
+
+__device__ __forceinline__ void flush_acc(const SearchParams& p, uint32_t t, uint32_t lane, TaskAcc& acc) {
+  if (lane == 0) {
+    if (acc.cnt) {
+      const unsigned long long old = atomicAdd(&p.count[t], acc.cnt);
+      if (p.cap && old + acc.cnt >= p.cap) p.stop[t] = 1u;
+    }
+    if (p.want_hash && acc.hash) atomicAdd(&p.hash[t], acc.hash);
+    if (acc.bytes) atomicAdd(&p.bytes[t], acc.bytes);
+  }
+  acc = TaskAcc{0, 0, 0};
+  __syncwarp();
+}
+
+// Root task: positions 0 and 1 are the updated edge; level 1 holds the driver
+// segment of position 2.
+__device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, const Task& T,
+                         TaskAcc& acc) {
+  const uint32_t n = p.plan->n;
+  const uint32_t t = T.upd;
+  const PlanAnchor* A = &p.plan->anchors[T.anchor];
+  const UpdInfo U = p.info[t];
+  const uint32_t m0 = T.orient ? U.v2 : U.v1, m1 = T.orient ? U.v1 : U.v2;
+  if (n == 2) {
+    if (lane == 0) {
+      acc.cnt += 1;
+      if (p.want_hash) acc.hash += mix64(pair_hash(A->pos[0].qv, m0) + pair_hash(A->pos[1].qv, m1));
+    }
+    return;
+  }
+  const PlanPos P2 = A->pos[2];
+  uint32_t sz = 0xffffffffu, szt = 1;
+  uint64_t lo = 0, hi = 0;
+  unsigned long long rb = 0;
+  if (lane < P2.nb) {
+    const uint32_t j = A->back_pos[P2.boff + lane], c = A->back_combo[P2.boff + lane];
+    const uint32_t v = j == 0 ? m0 : m1;
+    segment(p.g, v, c, lo, hi);
+    sz = (uint32_t)(hi - lo);
+    szt = seg_size_at(p.g, v, c, lo, hi, (int32_t)t);
+    rb = 4ull * szt;
+  }
+  const bool root_empty = __any_sync(0xffffffffu, szt == 0);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) rb += __shfl_xor_sync(0xffffffffu, rb, o);
+  acc.bytes += rb;
+  uint64_t key = ((uint64_t)sz << 32) | lane;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    uint64_t other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  const uint32_t minsz = root_empty ? 0u : (uint32_t)(key >> 32), sel = (uint32_t)key;
+  const uint32_t dlo0 = (uint32_t)__shfl_sync(0xffffffffu, lo, sel);
+  if (minsz == 0) return;
+  if (lane == 0) {
+    lv[1].cnt = 1; lv[1].cur_e = 0; lv[1].cur_k = 0;
+    lv[1].dlo[0] = dlo0; lv[1].dn[0] = minsz; lv[1].dsel[0] = (uint8_t)sel;
+  }
+  __syncwarp();
+  run_levels(p, pool, lv, 1, lane, T, A, m0, m1, acc);
+}
+
+// Donated task: rebuild the chain of the partial match (exhausted levels
+// 1 .. depth-1) and continue from level `depth`.  The record is read through
+// L2 (ld.global.cg): records share cache lines with neighbouring slots that
+// this SM may have cached before they were written.
+__device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane,
+                            const DTask* D, uint32_t B, TaskAcc& acc, uint32_t& upd_out) {
+  const uint32_t* Dw = reinterpret_cast<const uint32_t*>(D);
+  const uint32_t hw = lane < 5 ? __ldcg(Dw + lane) : 0u;  // upd, anchor|orient|depth, dlo, dn, dsel
+  const uint32_t mv = __ldcg(Dw + 5 + lane);               // m[lane]
+  const uint32_t upd = __shfl_sync(0xffffffffu, hw, 0);
+  const uint32_t w1 = __shfl_sync(0xffffffffu, hw, 1);
+  const uint32_t dlo = __shfl_sync(0xffffffffu, hw, 2);
+  const uint32_t dn = __shfl_sync(0xffffffffu, hw, 3);
+  const uint32_t dsel = __shfl_sync(0xffffffffu, hw, 4);
+  const uint32_t anchor = w1 & 0xffffu, orient = (w1 >> 16) & 0xffu, depth = w1 >> 24;
+  const uint32_t n = p.plan->n;
+  upd_out = upd;
+  if (upd >= B || anchor >= p.plan->n_anchor || depth < 1 || depth + 2 > n || dn == 0) {
+    if (lane == 0) atomicExch(p.error, kErrBadTask);
+    return;
+  }
+  Task T{upd, (uint16_t)anchor, (uint8_t)orient, 0};
+  const PlanAnchor* A = &p.plan->anchors[anchor];
+  const uint32_t m0 = __shfl_sync(0xffffffffu, mv, 0), m1 = __shfl_sync(0xffffffffu, mv, 1);
+  for (uint32_t L = 1; L <= depth; L++) {
+    const uint32_t v = __shfl_sync(0xffffffffu, mv, L);
+    if (lane == 0) {
+      LevelSM& S = lv[L];
+      S.cnt = 1; S.cur_k = 0; S.v[0] = v; S.par[0] = 0;
+      S.cur_e = (L < depth) ? 1u : 0u;
+      if (L == depth) { S.dlo[0] = dlo; S.dn[0] = dn; S.dsel[0] = (uint8_t)dsel; }
+    }
+  }
+  __syncwarp();
+  if (p.stop[upd]) return;
+  run_levels(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
+}
+
+__global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint32_t task_cap, uint32_t qcap) {
+  q->donated += min(q->tail, qcap);  // tasks handed over by the previous launch
+  q->head = 0; q->tail = 0; q->idle = 0;
+  q->pending = min(*n_tasks, task_cap);
+}
+
 template <int W>
 __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -143,166 +427,63 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
   const uint32_t* pool = p.g.pools[p.g.ps->active];
   const uint32_t ntask = min(*p.n_tasks, p.task_cap);
   volatile unsigned int* stop = p.stop;
+  TaskAcc acc{0, 0, 0};
 
+  // 1. root tasks, in claim order
   for (;;) {
     uint32_t ti = 0;
     if (lane == 0) ti = atomicAdd(p.task_next, 1u);
     ti = __shfl_sync(0xffffffffu, ti, 0);
     if (ti >= ntask) break;
     const Task T = p.tasks[ti];
-    const uint32_t t = T.upd;
-    if (stop[t]) continue;
-    const PlanAnchor* A = &p.plan->anchors[T.anchor];
-    const UpdInfo U = p.info[t];
-    const uint32_t m0 = T.orient ? U.v2 : U.v1, m1 = T.orient ? U.v1 : U.v2;
-    unsigned long long cnt_local = 0, hash_local = 0, bytes_local = 0;
-
-    if (n == 2) {
-      if (lane == 0) {
-        cnt_local = 1;
-        if (p.want_hash) hash_local = mix64(pair_hash(A->pos[0].qv, m0) + pair_hash(A->pos[1].qv, m1));
-      }
-    } else {
-      // driver of position 2 for the root (positions 0 and 1 matched)
-      const PlanPos P2 = A->pos[2];
-      uint32_t sz = 0xffffffffu, szt = 1;
-      uint64_t lo = 0, hi = 0;
-      unsigned long long rb = 0;
-      if (lane < P2.nb) {
-        const uint32_t j = A->back_pos[P2.boff + lane], c = A->back_combo[P2.boff + lane];
-        const uint32_t v = j == 0 ? m0 : m1;
-        segment(p.g, v, c, lo, hi);
-        sz = (uint32_t)(hi - lo);
-        szt = seg_size_at(p.g, v, c, lo, hi, (int32_t)t);
-        rb = 4ull * szt;
-      }
-      const bool root_empty = __any_sync(0xffffffffu, szt == 0);
-#pragma unroll
-      for (int o = 16; o; o >>= 1) rb += __shfl_xor_sync(0xffffffffu, rb, o);
-      bytes_local += rb;
-      uint64_t key = ((uint64_t)sz << 32) | lane;
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        uint64_t other = __shfl_xor_sync(0xffffffffu, key, o);
-        key = other < key ? other : key;
-      }
-      const uint32_t minsz = root_empty ? 0u : (uint32_t)(key >> 32), sel = (uint32_t)key;
-      const uint32_t dlo0 = (uint32_t)__shfl_sync(0xffffffffu, lo, sel);
-      if (minsz != 0) {
-        if (lane == 0) {
-          lv[1].cnt = 1; lv[1].cur_e = 0; lv[1].cur_k = 0;
-          lv[1].dlo[0] = dlo0; lv[1].dn[0] = minsz; lv[1].dsel[0] = (uint8_t)sel;
-        }
-        __syncwarp();
-        int d = 1;
-        uint32_t iter = 0;
-        while (d >= 1) {
-          if ((++iter & 7) == 0) {
-            uint32_t st = (lane == 0) ? stop[t] : 0u;
-            if (__shfl_sync(0xffffffffu, st, 0)) break;
-          }
-          LevelSM& L = lv[d];
-          const uint32_t cnt = L.cnt, ce = L.cur_e, ck = L.cur_k;
-          if (ce >= cnt) { d--; continue; }
-          // the next 32 (entry, driver element) pairs of this level
-          const uint32_t el = ce + lane;
-          const uint32_t rem = (el < cnt) ? L.dn[el] - (lane == 0 ? ck : 0u) : 0u;
-          const uint32_t incl = warp_incl_scan(rem, lane);
-          const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-          uint32_t owner = 0;
-#pragma unroll
-          for (uint32_t step = 16; step; step >>= 1) {
-            const uint32_t v = __shfl_sync(0xffffffffu, incl, owner + step - 1);
-            if (v <= lane) owner += step;
-          }
-          const uint32_t prev = __shfl_sync(0xffffffffu, incl, owner > 0 ? (owner - 1) & 31 : 0);
-          const bool active = lane < total;
-          const uint32_t e = ce + owner;
-          const uint32_t kk = lane - (owner > 0 ? prev : 0u) + (owner == 0 ? ck : 0u);
-          uint32_t nce, nck;
-          if (total <= 32) {
-            nce = ce + min(32u, cnt - ce); nck = 0;
-          } else {
-            const uint32_t o31 = __shfl_sync(0xffffffffu, owner, 31);
-            const uint32_t k31 = __shfl_sync(0xffffffffu, kk, 31);
-            const uint32_t e31 = ce + o31;
-            if (k31 + 1 >= L.dn[e31]) { nce = e31 + 1; nck = 0; } else { nce = e31; nck = k31 + 1; }
-          }
-          const uint32_t pos = (uint32_t)d + 1;
-          bool valid = false;
-          uint32_t x = 0, ndlo = 0, ndn = 0, ndsel = 0;
-          unsigned long long nb4 = 0;
-          uint32_t m[kMaxQ];
-          if (active) {
-            x = pool[(uint64_t)L.dlo[e] + kk];
-            m[0] = m0; m[1] = m1;
-            uint32_t idx = e;
-            for (int l2 = d; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
-            valid = check_candidate(p, pool, A, pos, x, m, L.dsel[e], (int32_t)t);
-            if (valid && pos + 1 < n) {
-              m[pos] = x;
-              valid = pick_driver(p, A, pos + 1, m, (int32_t)t, ndlo, ndn, ndsel, nb4);
-            }
-          }
-          __syncwarp();
-          if (lane == 0) { L.cur_e = nce; L.cur_k = nck; }
-          const uint32_t mask = __ballot_sync(0xffffffffu, valid);
-          if (pos + 1 < n) {
-#pragma unroll
-            for (int o = 16; o; o >>= 1) nb4 += __shfl_xor_sync(0xffffffffu, nb4, o);
-            bytes_local += nb4;
-          }
-          if (pos == n - 1) {
-            const uint32_t c = __popc(mask);
-            if (p.want_hash) {
-              unsigned long long h = 0;
-              if (valid) {
-                uint64_t s = pair_hash(A->pos[pos].qv, x);
-                for (uint32_t q = 0; q < pos; q++) s += pair_hash(A->pos[q].qv, m[q]);
-                h = mix64(s);
-              }
-#pragma unroll
-              for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-              hash_local += h;
-            }
-            cnt_local += c;
-            if (c && p.cap) {
-              unsigned int hit = 0;
-              if (lane == 0) {
-                const unsigned long long old = atomicAdd(&p.count[t], cnt_local);
-                cnt_local = 0;
-                if (old + c >= p.cap) { stop[t] = 1u; hit = 1; }
-              }
-              if (__shfl_sync(0xffffffffu, hit, 0)) break;
-            }
-          } else {
-            LevelSM& N = lv[pos];
-            if (valid) {
-              const uint32_t slot = __popc(mask & ((1u << lane) - 1u));
-              N.v[slot] = x; N.par[slot] = (uint8_t)e; N.dlo[slot] = ndlo; N.dn[slot] = ndn;
-              N.dsel[slot] = (uint8_t)ndsel;
-            }
-            if (lane == 0) { N.cnt = __popc(mask); N.cur_e = 0; N.cur_k = 0; }
-            __syncwarp();
-            if (mask) d = (int)pos;
-          }
-        }
-      }
-    }
-    if (lane == 0) {
-      if (cnt_local) {
-        const unsigned long long old = atomicAdd(&p.count[t], cnt_local);
-        if (p.cap && old + cnt_local >= p.cap) stop[t] = 1u;
-      }
-      if (p.want_hash && hash_local) atomicAdd(&p.hash[t], hash_local);
-      if (bytes_local) atomicAdd(&p.bytes[t], bytes_local);
-    }
-    __syncwarp();
+    if (!stop[T.upd]) run_root(p, pool, lv, lane, T, acc);
+    flush_acc(p, T.upd, lane, acc);
+    if (lane == 0 && p.dq) atomicSub(&p.q->pending, 1u);
   }
+  if (!p.dq) return;
+  // 2. donated tasks until every task is done
+  volatile SearchQueue* q = p.q;
+  bool registered = false;
+  for (;;) {
+    unsigned int claimed = 0xffffffffu;
+    if (lane == 0) {
+      unsigned long long t0 = global_ns();
+      for (;;) {
+        const unsigned int h = q->head, tl = min(q->tail, p.qcap);
+        if (h < tl) {
+          if (atomicCAS(&p.q->head, h, h + 1) == h) { claimed = h; break; }
+          continue;
+        }
+        if (q->pending == 0) break;
+        if (!registered) { atomicAdd(&p.q->idle, 1u); registered = true; }
+        __nanosleep(1024);
+        if (global_ns() - t0 > p.wait_limit_ns) { atomicExch(p.error, kErrWaitTimeout); break; }
+      }
+      if (registered && claimed != 0xffffffffu) { atomicSub(&p.q->idle, 1u); registered = false; }
+      if (claimed != 0xffffffffu) {
+        // the donor reserved the slot before filling it: wait for its flag
+        unsigned long long t1 = global_ns();
+        while (*(volatile unsigned int*)(p.ready + claimed) != p.epoch) {
+          __nanosleep(64);
+          if (global_ns() - t1 > p.wait_limit_ns) { atomicExch(p.error, kErrWaitTimeout); claimed = 0xfffffffeu; break; }
+        }
+        __threadfence();
+      }
+    }
+    claimed = __shfl_sync(0xffffffffu, claimed, 0);
+    if (claimed == 0xffffffffu) break;
+    if (claimed == 0xfffffffeu) break;  // gave up waiting: error flagged
+    uint32_t t = 0;
+    run_donated(p, pool, lv, lane, p.dq + claimed, p.batch, acc, t);
+    if (t < p.batch) flush_acc(p, t, lane, acc);
+    if (lane == 0) atomicSub(&p.q->pending, 1u);
+  }
+  if (lane == 0 && registered) atomicSub(&p.q->idle, 1u);
 }
 
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s) {
   const size_t smem = search_smem_bytes(n_q, warps);
+  if (p.q) k_search_prep<<<1, 1, 0, s>>>(p.q, p.n_tasks, p.task_cap, p.qcap);
   switch (warps) {
     case 4:
       cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -350,7 +531,8 @@ __global__ void k_classify(uint64_t n, const csm_update* ups, DevGraph g, const 
     const uint32_t L1 = g.vlabel[u.id1], L2 = g.vlabel[u.id2];
     for (uint32_t a = 0; a < plan->n_anchor && sf; a++) {
       const PlanAnchor* A = &plan->anchors[a];
-      if (A->el == u.label && ((A->la == L1 && A->lb == L2) || (A->la == L2 && A->lb == L1))) sf = 0;
+      const uint32_t el = fold_elabel(g, u.label);
+      if (A->el == el && ((A->la == L1 && A->lb == L2) || (A->la == L2 && A->lb == L1))) sf = 0;
     }
   }
   safe[i] = sf;
