@@ -115,6 +115,11 @@ typedef struct csm_stats {
   uint64_t search_launches;   /* launches of the search kernel */
   double search_ms;           /* their summed duration, from CUDA events on the launching stream */
   uint64_t work_bytes;        /* algorithmic bytes of all completed updates (csm_result.work_bytes) */
+  uint64_t search_busy_ns;    /* summed warp time inside search tasks */
+  uint64_t search_idle_ns;    /* summed warp time waiting for handed-over tasks */
+  uint64_t search_iters;      /* chunk iterations (32 candidate slots each) */
+  uint64_t search_donations;  /* hand-overs of work between warps */
+  uint64_t search_starved;    /* idle warps were waiting but a busy warp had nothing to hand over */
 } csm_stats;
 
 typedef struct csm_ctx csm_ctx;
@@ -174,6 +179,13 @@ int csm_gpu_results(csm_ctx* ctx, uint64_t first_seq, uint64_t n, csm_result* ou
 int csm_gpu_results_device(csm_ctx* ctx, const csm_result** d_out, uint64_t* n);
 
 int csm_gpu_stats(csm_ctx* ctx, csm_stats* out);
+
+/* Search tracing counters, cumulative over the context's search launches:
+ * out[0] busy ns, [1] idle ns, [2] chunk iterations, [3] hand-overs,
+ * [4] starved checks, [5] hand-over checks, [6] checks that saw idle warps,
+ * [7] ns in root tasks, [8] latest root-task end after its launch start (max),
+ * [9] longest task ns (max).  Writes min(n, 10) values; waits for the stream. */
+int csm_gpu_search_counters(csm_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* Number of distinct kernel launches issued by this context so far. */
 uint64_t csm_gpu_kernel_launches(csm_ctx* ctx);

@@ -77,6 +77,8 @@ class CsmStats(C.Structure):
         ("last_batch_ms", C.c_double), ("total_device_ms", C.c_double),
         ("index_entries", C.c_uint64), ("index_vertices", C.c_uint64),
         ("search_launches", C.c_uint64), ("search_ms", C.c_double), ("work_bytes", C.c_uint64),
+        ("search_busy_ns", C.c_uint64), ("search_idle_ns", C.c_uint64), ("search_iters", C.c_uint64),
+        ("search_donations", C.c_uint64), ("search_starved", C.c_uint64),
     ]
 
 
@@ -96,6 +98,7 @@ _SIGNATURES = [
     ("csm_gpu_results_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     ("csm_gpu_stats", C.c_int, [C.c_void_p, C.POINTER(CsmStats)]),
     ("csm_gpu_stream", C.c_void_p, [C.c_void_p]),
+    ("csm_gpu_search_counters", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("csm_gpu_kernel_launches", C.c_uint64, [C.c_void_p]),
     ("csm_gpu_destroy", None, [C.c_void_p]),
     ("csm_gpu_last_error", C.c_char_p, []),

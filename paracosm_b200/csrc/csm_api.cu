@@ -98,8 +98,9 @@ struct csm_ctx {
   unsigned long long* d_stamp = nullptr;  // [0] submit time (globaltimer)
   SearchQueue* d_q = nullptr;
   DTask* d_dq = nullptr;
-  unsigned int* d_ready = nullptr;
-  uint32_t qcap = 0, epoch = 0;
+  unsigned long long* d_qseq = nullptr;
+  uint32_t qcap = 0;
+  SearchStats* d_sstat = nullptr;
   csm_result* d_results = nullptr; uint64_t results_cap = 0;
   void* d_cub = nullptr; size_t cub_bytes = 0;
   // bookkeeping
@@ -243,12 +244,19 @@ static int ensure_batch_buffers(csm_ctx* ctx) {
   AL(ctx->d_count, 8ull * B); AL(ctx->d_hash, 8ull * B); AL(ctx->d_bytes, 8ull * B);
   AL(ctx->d_stop, 4ull * B); AL(ctx->d_safe, 4ull * B);
   AL(ctx->d_stamp, 64);
-  ctx->qcap = 1u << 20;
+  ctx->qcap = 1u << 16;  // outstanding handed-over tasks never exceed the idle warps
   AL(ctx->d_q, sizeof(SearchQueue));
+  AL(ctx->d_sstat, sizeof(SearchStats));
+  CK(cudaMemsetAsync(ctx->d_sstat, 0, sizeof(SearchStats), ctx->st));
   AL(ctx->d_dq, sizeof(DTask) * (size_t)ctx->qcap);
-  AL(ctx->d_ready, 4ull * ctx->qcap);
+  AL(ctx->d_qseq, 8ull * ctx->qcap);
   CK(cudaMemsetAsync(ctx->d_q, 0, sizeof(SearchQueue), ctx->st));
-  CK(cudaMemsetAsync(ctx->d_ready, 0, 4ull * ctx->qcap, ctx->st));
+  {
+    std::vector<unsigned long long> seq(ctx->qcap);
+    for (uint32_t i = 0; i < ctx->qcap; i++) seq[i] = i;
+    CK(cudaMemcpyAsync(ctx->d_qseq, seq.data(), 8ull * ctx->qcap, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
 #undef AL
   // CUB scratch: the largest of the sorts issued per batch
   size_t b1 = 0, b2 = 0, b3 = 0;
@@ -354,9 +362,12 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash; sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
   sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = ctx->cfg.max_results;
   sp.homo = ctx->cfg.homomorphism; sp.want_hash = ctx->cfg.want_hash; sp.error = &g.ps->error;
-  sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.ready = ctx->d_ready; sp.qcap = ctx->qcap; sp.epoch = ++ctx->epoch;
-  sp.wait_limit_ns = 600ull * 1000000000ull;
+  sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.qseq = ctx->d_qseq; sp.qcap = ctx->qcap;
+  sp.wait_limit_ns = 30ull * 1000000000ull;
+  sp.slot_limit_ns = 100ull * 1000000ull;
+  sp.task_limit_ns = 20ull * 1000000000ull;
   sp.batch = B;
+  sp.sstat = ctx->d_sstat;
   uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
@@ -441,13 +452,47 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
   return CSM_OK;
 }
 
+// Puts the hand-over ring back into its initial state (after a failed launch).
+static int reset_ring(csm_ctx* ctx) {
+  if (!ctx->d_q) return CSM_OK;
+  CK(cudaMemsetAsync(ctx->d_q, 0, sizeof(SearchQueue), ctx->st));
+  std::vector<unsigned long long> seq(ctx->qcap);
+  for (uint32_t i = 0; i < ctx->qcap; i++) seq[i] = i;
+  CK(cudaMemcpyAsync(ctx->d_qseq, seq.data(), 8ull * ctx->qcap, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return CSM_OK;
+}
+
 static int check_device_error(csm_ctx* ctx) {
   PoolState ps;
   CK(cudaMemcpy(&ps, ctx->g.ps, sizeof(PoolState), cudaMemcpyDeviceToHost));
   if (ps.error) {
     static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow",
-                                  "search queue wait limit", "malformed donated task"};
-    return set_err(CSM_EDEVICE, "device error %u (%s)", ps.error, ps.error < 6 ? names[ps.error] : "?");
+                                  "search queue wait limit", "malformed donated task", "ring left undrained",
+                                  "task time guard"};
+    char extra[256] = "";
+    if (ctx->d_sstat) {
+      SearchStats ss;
+      if (cudaMemcpy(&ss, ctx->d_sstat, sizeof(ss), cudaMemcpyDeviceToHost) == cudaSuccess) {
+        if (ss.bad_set)
+          snprintf(extra, sizeof(extra), " [ticket %llu seq %llu words %u %08x %u %u %u batch %u]", ss.bad_ticket,
+                   ss.bad_seq, ss.bad_words[0], ss.bad_words[1], ss.bad_words[2], ss.bad_words[3], ss.bad_words[4],
+                   ss.bad_batch);
+        if (ss.guard_set) {
+          int o = snprintf(extra, sizeof(extra), " [guard d %u upd %u iters %llu lv", ss.guard_d, ss.guard_upd,
+                           ss.guard_iters);
+          for (unsigned L = 0; L < ss.guard_d && L < 16 && o < (int)sizeof(extra) - 40; L++)
+            o += snprintf(extra + o, sizeof(extra) - o, " %u/%u/%u/%u", ss.guard_lv[4 * L], ss.guard_lv[4 * L + 1],
+                          ss.guard_lv[4 * L + 2], ss.guard_lv[4 * L + 3]);
+          snprintf(extra + o, sizeof(extra) - o, "]");
+        }
+      }
+    }
+    const unsigned int code = ps.error;
+    ps.error = 0;
+    cudaMemcpy(ctx->g.ps, &ps, sizeof(PoolState), cudaMemcpyHostToDevice);
+    reset_ring(ctx);
+    return set_err(CSM_EDEVICE, "device error %u (%s)%s", code, code < 8 ? names[code] : "?", extra);
   }
   return CSM_OK;
 }
@@ -824,7 +869,11 @@ int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
   if (ctx->d_q) {
     SearchQueue q;
     CK(cudaMemcpy(&q, ctx->d_q, sizeof(q), cudaMemcpyDeviceToHost));
-    out->donated_tasks = q.donated + std::min<uint64_t>(q.tail, ctx->qcap);
+    out->donated_tasks = q.tail;
+    SearchStats ss;
+    CK(cudaMemcpy(&ss, ctx->d_sstat, sizeof(ss), cudaMemcpyDeviceToHost));
+    out->search_busy_ns = ss.busy_ns; out->search_idle_ns = ss.idle_ns; out->search_iters = ss.iters;
+    out->search_donations = ss.donations; out->search_starved = ss.starved;
   }
   out->search_launches = ctx->search_launches;
   out->search_ms = ctx->search_ms;
@@ -835,6 +884,18 @@ int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
 uint64_t csm_gpu_kernel_launches(csm_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 void* csm_gpu_stream(csm_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+
+int csm_gpu_search_counters(csm_ctx* ctx, uint64_t* out, uint32_t n) {
+  if (!ctx || (n && !out)) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->d_sstat) { for (uint32_t i = 0; i < n; i++) out[i] = 0; return CSM_OK; }
+  CK(cudaStreamSynchronize(ctx->st));
+  SearchStats ss;
+  CK(cudaMemcpy(&ss, ctx->d_sstat, sizeof(ss), cudaMemcpyDeviceToHost));
+  const uint64_t v[10] = {ss.busy_ns, ss.idle_ns, ss.iters, ss.donations, ss.starved, ss.checks, ss.checks_hungry,
+                          ss.root_busy_ns, ss.last_root_ns, ss.max_task_ns};
+  for (uint32_t i = 0; i < n && i < 10; i++) out[i] = v[i];
+  return CSM_OK;
+}
 
 void csm_gpu_destroy(csm_ctx* ctx) {
   if (!ctx) return;

@@ -61,11 +61,36 @@ struct DTask {
 };
 static_assert(sizeof(DTask) == 160, "DTask is 160 bytes");
 
-// Work queue of one search launch.  `pending` counts tasks (root and
-// donated) not finished yet; idle warps exit when it reaches zero.
+// Work queue of the search launches.  Tickets (head, tail) count up across
+// launches; `pending` counts this launch's tasks (root and donated) that are
+// not finished, and idle warps exit when it reaches zero; `hungry` counts idle
+// warps not yet promised a task, which caps how much busy warps hand over.
 struct SearchQueue {
-  unsigned int head, tail, idle, pending;
-  unsigned long long donated;  // tasks handed over by earlier launches
+  unsigned long long head, tail;
+  unsigned int hungry, pending;
+};
+
+// Cumulative search counters (device memory, read by csm_gpu_stats).
+struct SearchStats {
+  unsigned long long busy_ns;    // warp time spent inside tasks
+  unsigned long long idle_ns;    // warp time spent waiting for handed-over tasks
+  unsigned long long iters;      // chunk iterations (32 candidate slots each)
+  unsigned long long donations;  // hand-overs (one or more tasks each)
+  unsigned long long starved;    // idle warps existed but nothing could be handed over
+  unsigned long long checks;     // hand-over checks made by busy warps
+  unsigned long long checks_hungry;  // ... that saw idle warps waiting
+  unsigned long long root_busy_ns;   // warp time in root tasks (the rest is handed-over tasks)
+  unsigned long long last_root_ns;   // max over warps: kernel start -> end of its last root task
+  unsigned long long max_task_ns;    // longest single task
+  unsigned long long launch_t0;      // globaltimer at the start of the current launch
+  // first malformed handed-over record seen: ticket, observed sequence, words 0..4, batch
+  unsigned long long bad_ticket, bad_seq;
+  unsigned int bad_words[5], bad_batch;
+  unsigned int bad_set, pad_;
+  // first task stopped by the task time guard: its depth, iterations, update and level cursors
+  unsigned int guard_set, guard_d, guard_upd, guard_pad;
+  unsigned long long guard_iters;
+  unsigned int guard_lv[4 * 16];  // per level 1..16: cnt, cur_e, cur_k, dn[cur_e]
 };
 
 struct SearchParams {
@@ -88,12 +113,14 @@ struct SearchParams {
   unsigned int* error;
   // work donation (null dq: off)
   SearchQueue* q;
-  DTask* dq;
-  unsigned int* ready;        // ready[i] == epoch once dq[i] is filled
+  DTask* dq;                  // ring of qcap slots (a power of two)
+  unsigned long long* qseq;   // per-slot sequence numbers
   uint32_t qcap;
-  uint32_t epoch;
-  unsigned long long wait_limit_ns;
+  unsigned long long wait_limit_ns;  // idle warps waiting for work
+  unsigned long long slot_limit_ns;  // a hand-over waiting for its ring slot
+  unsigned long long task_limit_ns;  // one task (a guard: a correct walk always ends)
   uint32_t batch;             // updates in this batch (bound of task update indices)
+  SearchStats* sstat;
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,

@@ -141,7 +141,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Per-task accumulators, flushed to the update's counters when the task ends.
 struct TaskAcc {
-  unsigned long long cnt, hash, bytes;
+  unsigned long long cnt, hash, bytes, iters, checks, checks_hungry;
 };
 
 // Hands unexpanded work at the shallowest level with work left to idle warps:
@@ -151,28 +151,45 @@ struct TaskAcc {
 // position L + 1.  Returns the number of tasks handed over.
 __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t lane, uint32_t idle_now,
                            uint32_t t, const Task& T, uint32_t m0, uint32_t m1) {
+  // Ranges are split down to two elements near the root (where every element
+  // heads a large subtree) and only from 64 elements further down.
+  const int n = (int)p.plan->n;
   int Ls = 0;
   uint32_t mode = 0;  // 1: whole entries, 2: split the entry in progress
-  for (int L = 1; L <= d; L++) {
+  for (int L = 1; L <= d && L <= n - 2; L++) {
     const uint32_t cnt = lv[L].cnt, ce = lv[L].cur_e;
     if (ce >= cnt) continue;
     if (cnt - ce >= 2) { Ls = L; mode = 1; break; }
-    if (lv[L].dn[ce] - lv[L].cur_k >= 64) { Ls = L; mode = 2; break; }
+    const uint32_t min_split = (L + 5 <= n) ? 2u : 64u;
+    if (lv[L].dn[ce] - lv[L].cur_k >= min_split) { Ls = L; mode = 2; break; }
   }
-  if (!mode) return 0;
+  if (!mode) {
+    if (lane == 0) atomicAdd(&p.sstat->starved, 1ULL);
+    return 0;
+  }
   LevelSM& S = lv[Ls];
   const uint32_t cnt = S.cnt, ce = S.cur_e;
-  uint32_t k = mode == 1 ? min(min(idle_now, cnt - ce - 1), 32u) : 1u;
-  unsigned int base = 0;
+  const uint32_t avail = mode == 1 ? min(cnt - ce - 1, 32u) : 1u;
+  // take up to `avail` units of hunger (idle warps not yet promised a task)
+  unsigned long long base = 0;
+  uint32_t k = 0;
   if (lane == 0) {
-    base = atomicAdd(&p.q->tail, k);
-    const unsigned int ok = base >= p.qcap ? 0u : min(k, p.qcap - base);
-    if (ok) atomicAdd(&p.q->pending, ok);
-    k = ok;
+    unsigned int h = *(volatile unsigned int*)&p.q->hungry;
+    while (h) {
+      const unsigned int want = min(h, min(avail, idle_now));
+      const unsigned int prev = atomicCAS(&p.q->hungry, h, h - want);
+      if (prev == h) { k = want; break; }
+      h = prev;
+    }
+    if (k) {
+      atomicAdd(&p.q->pending, k);
+      base = atomicAdd(&p.q->tail, (unsigned long long)k);
+      atomicAdd(&p.sstat->donations, 1ULL);
+    }
   }
-  base = __shfl_sync(0xffffffffu, base, 0);
   k = __shfl_sync(0xffffffffu, k, 0);
   if (k == 0) return 0;
+  base = __shfl_sync(0xffffffffu, base, 0);
   // entry handed to lane j and its driver range
   uint32_t e = 0, dlo = 0, dn = 0;
   if (mode == 1) {
@@ -185,21 +202,31 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
     dn = rem - keep;
   }
   if (lane < k) {
-    DTask* D = p.dq + base + lane;
+    const unsigned long long ticket = base + lane;
+    const uint32_t slot = (uint32_t)(ticket & (p.qcap - 1));
+    // the slot is free for this ticket once its previous reader released it
+    volatile unsigned long long* sq = p.qseq + slot;
+    const unsigned long long t0 = global_ns();
+    bool ok = true;
+    while (*sq != ticket) {
+      __nanosleep(64);
+      if (global_ns() - t0 > p.slot_limit_ns) { atomicExch(p.error, kErrWaitTimeout); ok = false; break; }
+    }
+    DTask* D = p.dq + slot;
     uint32_t idx = e;
     for (int L = Ls; L >= 2; --L) { D->m[L] = lv[L].v[idx]; idx = lv[L].par[idx]; }
     D->m[0] = m0; D->m[1] = m1;
-    D->upd = t; D->anchor = T.anchor; D->orient = T.orient; D->depth = (uint8_t)Ls;
+    D->upd = ok ? t : 0xffffffffu;  // a record that could not be placed is published as void
+    D->anchor = T.anchor; D->orient = T.orient; D->depth = (uint8_t)Ls;
     D->dlo = dlo; D->dn = dn; D->dsel = S.dsel[e];
+    __threadfence();
+    *sq = ticket + 1;  // publish
   }
   __syncwarp();
   if (lane == 0) {
     if (mode == 1) S.cnt = cnt - k;
     else S.dn[ce] = S.cur_k + ((S.dn[ce] - S.cur_k) >> 1);
   }
-  __threadfence();
-  __syncwarp();
-  if (lane < k) *(volatile unsigned int*)(p.ready + base + lane) = p.epoch;
   __syncwarp();
   return k;
 }
@@ -212,20 +239,43 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
   const uint32_t t = T.upd;
   volatile unsigned int* stop = p.stop;
   uint32_t iter = 0;
+  const unsigned long long t_start = global_ns();
   while (d >= 1) {
     ++iter;
+    if ((iter & 63) == 0) {
+      unsigned int expired = (lane == 0) ? (global_ns() - t_start > p.task_limit_ns) : 0u;
+      if (__shfl_sync(0xffffffffu, expired, 0)) {
+        if (lane == 0) {
+          atomicExch(p.error, kErrTaskGuard);
+          if (atomicCAS(&p.sstat->guard_set, 0u, 1u) == 0u) {
+            p.sstat->guard_d = (unsigned)d; p.sstat->guard_upd = t; p.sstat->guard_iters = iter;
+            for (int L = 1; L <= d && L <= 16; L++) {
+              const uint32_t ce = lv[L].cur_e;
+              p.sstat->guard_lv[4 * (L - 1) + 0] = lv[L].cnt;
+              p.sstat->guard_lv[4 * (L - 1) + 1] = ce;
+              p.sstat->guard_lv[4 * (L - 1) + 2] = lv[L].cur_k;
+              p.sstat->guard_lv[4 * (L - 1) + 3] = ce < 32 ? lv[L].dn[ce] : 0xffffffffu;
+            }
+          }
+        }
+        break;
+      }
+    }
     if ((iter & 7) == 0) {
       uint32_t st = (lane == 0) ? stop[t] : 0u;
       if (__shfl_sync(0xffffffffu, st, 0)) break;
     }
-    if ((iter & 15) == 0 && p.dq) {
-      uint32_t idle_now = (lane == 0) ? *(volatile unsigned int*)&p.q->idle : 0u;
+    if ((iter & 3) == 0 && p.dq) {
+      uint32_t idle_now = (lane == 0) ? *(volatile unsigned int*)&p.q->hungry : 0u;
       idle_now = __shfl_sync(0xffffffffu, idle_now, 0);
+      acc.checks++;
+      if (idle_now) acc.checks_hungry++;
       if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1);
     }
     LevelSM& L = lv[d];
     const uint32_t cnt = L.cnt, ce = L.cur_e, ck = L.cur_k;
     if (ce >= cnt) { d--; continue; }
+    acc.iters++;
     // the next 32 (entry, driver element) pairs of this level
     const uint32_t el = ce + lane;
     const uint32_t rem = (el < cnt) ? L.dn[el] - (lane == 0 ? ck : 0u) : 0u;
@@ -255,7 +305,12 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     uint32_t x = 0, ndlo = 0, ndn = 0, ndsel = 0;
     unsigned long long nb4 = 0;
     uint32_t m[kMaxQ];
-    if (active) {
+    bool act = active;
+    if (act && (e >= cnt || kk >= L.dn[e])) {  // lanes disagree on the level state: flag it, read nothing
+      atomicExch(p.error, kErrBadTask);
+      act = false;
+    }
+    if (act) {
       x = pool[(uint64_t)L.dlo[e] + kk];
       m[0] = m0; m[1] = m1;
       uint32_t idx = e;
@@ -268,6 +323,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     }
     __syncwarp();
     if (lane == 0) { L.cur_e = nce; L.cur_k = nck; }
+    __syncwarp();  // the cursor must be visible to every lane before the next iteration reads it
     const uint32_t mask = __ballot_sync(0xffffffffu, valid);
     if (pos + 1 < n) {
 #pragma unroll
@@ -320,7 +376,7 @@ __device__ __forceinline__ void flush_acc(const SearchParams& p, uint32_t t, uin
     if (p.want_hash && acc.hash) atomicAdd(&p.hash[t], acc.hash);
     if (acc.bytes) atomicAdd(&p.bytes[t], acc.bytes);
   }
-  acc = TaskAcc{0, 0, 0};
+  acc.cnt = 0; acc.hash = 0; acc.bytes = 0;
   __syncwarp();
 }
 
@@ -374,14 +430,11 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
 }
 
 // Donated task: rebuild the chain of the partial match (exhausted levels
-// 1 .. depth-1) and continue from level `depth`.  The record is read through
-// L2 (ld.global.cg): records share cache lines with neighbouring slots that
-// this SM may have cached before they were written.
-__device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane,
-                            const DTask* D, uint32_t B, TaskAcc& acc, uint32_t& upd_out) {
-  const uint32_t* Dw = reinterpret_cast<const uint32_t*>(D);
-  const uint32_t hw = lane < 5 ? __ldcg(Dw + lane) : 0u;  // upd, anchor|orient|depth, dlo, dn, dsel
-  const uint32_t mv = __ldcg(Dw + 5 + lane);               // m[lane]
+// 1 .. depth-1) and continue from level `depth`.  `hw` holds record words
+// 0..4 in lanes 0..4 and `mv` holds m[lane] (see DTask).
+__device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, uint32_t hw,
+                            uint32_t mv, TaskAcc& acc, uint32_t& upd_out, unsigned long long ticket,
+                            unsigned long long seen_seq) {
   const uint32_t upd = __shfl_sync(0xffffffffu, hw, 0);
   const uint32_t w1 = __shfl_sync(0xffffffffu, hw, 1);
   const uint32_t dlo = __shfl_sync(0xffffffffu, hw, 2);
@@ -390,8 +443,18 @@ __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM
   const uint32_t anchor = w1 & 0xffffu, orient = (w1 >> 16) & 0xffu, depth = w1 >> 24;
   const uint32_t n = p.plan->n;
   upd_out = upd;
-  if (upd >= B || anchor >= p.plan->n_anchor || depth < 1 || depth + 2 > n || dn == 0) {
-    if (lane == 0) atomicExch(p.error, kErrBadTask);
+  if (upd == 0xffffffffu) return;  // void record (its donor flagged an error)
+  if (upd >= p.batch || anchor >= p.plan->n_anchor || depth < 1 || depth + 2 > n || dn == 0 ||
+      (unsigned long long)dlo + dn > p.g.pool_cap) {
+    if (lane == 0) {
+      atomicExch(p.error, kErrBadTask);
+      if (atomicCAS(&p.sstat->bad_set, 0u, 1u) == 0u) {
+        p.sstat->bad_ticket = ticket; p.sstat->bad_seq = seen_seq; p.sstat->bad_batch = p.batch;
+        p.sstat->bad_words[0] = upd; p.sstat->bad_words[1] = w1; p.sstat->bad_words[2] = dlo;
+        p.sstat->bad_words[3] = dn; p.sstat->bad_words[4] = dsel;
+      }
+    }
+    upd_out = 0xffffffffu;
     return;
   }
   Task T{upd, (uint16_t)anchor, (uint8_t)orient, 0};
@@ -407,19 +470,26 @@ __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM
     }
   }
   __syncwarp();
-  if (p.stop[upd]) return;
+  const unsigned int stopped =
+      __shfl_sync(0xffffffffu, lane == 0 ? *(volatile unsigned int*)(p.stop + upd) : 0u, 0);
+  if (stopped) return;
   run_levels(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
 }
 
-__global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint32_t task_cap, uint32_t qcap) {
-  q->donated += min(q->tail, qcap);  // tasks handed over by the previous launch
-  q->head = 0; q->tail = 0; q->idle = 0;
+// Per launch: tickets keep counting up across launches (the ring's slot
+// sequence numbers stay consistent); hunger and pending start afresh.
+__global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint32_t task_cap, SearchStats* ss,
+                              unsigned int* error) {
+  if (q->head != q->tail) atomicExch(error, kErrRingState);  // an earlier launch left the ring undrained
+  q->hungry = 0;
   q->pending = min(*n_tasks, task_cap);
+  ss->launch_t0 = global_ns();
 }
 
 template <int W>
 __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint4 task_scratch[W * 10];  // one 160-byte record per warp
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t n = p.plan->n;
   const uint32_t nlev = n > 2 ? n - 2 : 1;
@@ -427,7 +497,9 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
   const uint32_t* pool = p.g.pools[p.g.ps->active];
   const uint32_t ntask = min(*p.n_tasks, p.task_cap);
   volatile unsigned int* stop = p.stop;
-  TaskAcc acc{0, 0, 0};
+  TaskAcc acc{0, 0, 0, 0, 0, 0};
+  unsigned long long root_ns = 0, last_root = 0, max_task = 0;
+  unsigned long long busy_ns = 0, idle_ns = 0;
 
   // 1. root tasks, in claim order
   for (;;) {
@@ -436,54 +508,99 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
     ti = __shfl_sync(0xffffffffu, ti, 0);
     if (ti >= ntask) break;
     const Task T = p.tasks[ti];
-    if (!stop[T.upd]) run_root(p, pool, lv, lane, T, acc);
+    const unsigned long long tb = global_ns();
+    // stop flags change under our feet: one lane reads, the warp follows it
+    const unsigned int stopped = __shfl_sync(0xffffffffu, lane == 0 ? stop[T.upd] : 0u, 0);
+    if (!stopped) run_root(p, pool, lv, lane, T, acc);
+    const unsigned long long te = global_ns();
+    busy_ns += te - tb;
+    root_ns += te - tb;
+    last_root = te;
+    max_task = max(max_task, te - tb);
     flush_acc(p, T.upd, lane, acc);
     if (lane == 0 && p.dq) atomicSub(&p.q->pending, 1u);
   }
-  if (!p.dq) return;
-  // 2. donated tasks until every task is done
+  if (lane == 0) {
+    atomicAdd(&p.sstat->root_busy_ns, root_ns);
+    if (last_root) atomicMax(&p.sstat->last_root_ns, last_root - p.sstat->launch_t0);
+  }
+  if (!p.dq) {
+    if (lane == 0) { atomicAdd(&p.sstat->busy_ns, busy_ns); atomicAdd(&p.sstat->iters, acc.iters); }
+    return;
+  }
+  // 2. donated tasks until every task is done.  The queue is a bounded ring
+  // of DTask slots with per-slot sequence numbers: slot (ticket % qcap) holds
+  // ticket T's record once seq == T + 1, and is free for ticket T + qcap once
+  // its reader stores seq = T + qcap.
   volatile SearchQueue* q = p.q;
   bool registered = false;
   for (;;) {
-    unsigned int claimed = 0xffffffffu;
+    unsigned long long claimed = ~0ULL, seen = 0;
     if (lane == 0) {
-      unsigned long long t0 = global_ns();
+      const unsigned long long t0 = global_ns();
+      unsigned int nap = 64;
       for (;;) {
-        const unsigned int h = q->head, tl = min(q->tail, p.qcap);
-        if (h < tl) {
-          if (atomicCAS(&p.q->head, h, h + 1) == h) { claimed = h; break; }
+        const unsigned long long h = q->head;
+        const unsigned long long sv = *(volatile unsigned long long*)(p.qseq + (h & (p.qcap - 1)));
+        if (sv == h + 1) {
+          if (atomicCAS((unsigned long long*)&p.q->head, h, h + 1) == h) { claimed = h; seen = sv; break; }
           continue;
         }
         if (q->pending == 0) break;
-        if (!registered) { atomicAdd(&p.q->idle, 1u); registered = true; }
-        __nanosleep(1024);
+        if (!registered) { atomicAdd(&p.q->hungry, 1u); registered = true; }
+        __nanosleep(nap);
+        nap = min(nap * 2, 2048u);
         if (global_ns() - t0 > p.wait_limit_ns) { atomicExch(p.error, kErrWaitTimeout); break; }
       }
-      if (registered && claimed != 0xffffffffu) { atomicSub(&p.q->idle, 1u); registered = false; }
-      if (claimed != 0xffffffffu) {
-        // the donor reserved the slot before filling it: wait for its flag
-        unsigned long long t1 = global_ns();
-        while (*(volatile unsigned int*)(p.ready + claimed) != p.epoch) {
-          __nanosleep(64);
-          if (global_ns() - t1 > p.wait_limit_ns) { atomicExch(p.error, kErrWaitTimeout); claimed = 0xfffffffeu; break; }
-        }
-        __threadfence();
+      if (claimed != ~0ULL) {
+        // hungry = registered idle warps - published unclaimed tasks: a task taken
+        // by a warp that never registered was promised to a registered one, whose
+        // unit goes back into the count
+        if (!registered) atomicAdd(&p.q->hungry, 1u);
+        registered = false;
       }
+      idle_ns += global_ns() - t0;
     }
     claimed = __shfl_sync(0xffffffffu, claimed, 0);
-    if (claimed == 0xffffffffu) break;
-    if (claimed == 0xfffffffeu) break;  // gave up waiting: error flagged
+    if (claimed == ~0ULL) break;
+    // lane 0 copies the record through L2 (records share cache lines with other
+    // slots) into the warp's scratch, and only then frees the slot for reuse
+    uint4* scratch = task_scratch + warp * 10;
+    if (lane == 0) {
+      __threadfence();
+      const uint32_t slot = (uint32_t)(claimed & (p.qcap - 1));
+      const uint4* src = reinterpret_cast<const uint4*>(p.dq + slot);
+#pragma unroll
+      for (int i = 0; i < 10; i++) scratch[i] = __ldcg(src + i);
+      __threadfence();
+      *(volatile unsigned long long*)(p.qseq + slot) = claimed + p.qcap;
+    }
+    __syncwarp();
+    const uint32_t* Dw = reinterpret_cast<const uint32_t*>(scratch);
+    const uint32_t hw = lane < 5 ? Dw[lane] : 0u;
+    const uint32_t mv = Dw[5 + lane];
+    __syncwarp();
     uint32_t t = 0;
-    run_donated(p, pool, lv, lane, p.dq + claimed, p.batch, acc, t);
+    const unsigned long long tb = global_ns();
+    run_donated(p, pool, lv, lane, hw, mv, acc, t, claimed, seen);
+    busy_ns += global_ns() - tb;
+    max_task = max(max_task, global_ns() - tb);
     if (t < p.batch) flush_acc(p, t, lane, acc);
     if (lane == 0) atomicSub(&p.q->pending, 1u);
   }
-  if (lane == 0 && registered) atomicSub(&p.q->idle, 1u);
+  if (lane == 0) {
+    atomicAdd(&p.sstat->busy_ns, busy_ns);
+    atomicAdd(&p.sstat->idle_ns, idle_ns);
+    atomicAdd(&p.sstat->iters, acc.iters);
+    atomicAdd(&p.sstat->checks, acc.checks);
+    atomicAdd(&p.sstat->checks_hungry, acc.checks_hungry);
+    atomicMax(&p.sstat->max_task_ns, max_task);
+  }
 }
 
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s) {
   const size_t smem = search_smem_bytes(n_q, warps);
-  if (p.q) k_search_prep<<<1, 1, 0, s>>>(p.q, p.n_tasks, p.task_cap, p.qcap);
+  if (p.q) k_search_prep<<<1, 1, 0, s>>>(p.q, p.n_tasks, p.task_cap, p.sstat, p.error);
   switch (warps) {
     case 4:
       cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

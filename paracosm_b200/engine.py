@@ -134,6 +134,13 @@ class Engine:
         check(self.lib, self.lib.csm_gpu_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in CsmStats._fields_}
 
+    def search_counters(self) -> dict:
+        out = np.zeros(10, dtype=np.uint64)
+        check(self.lib, self.lib.csm_gpu_search_counters(self.h, _ptr(out), 10))
+        names = ["busy_ns", "idle_ns", "iters", "donations", "starved", "checks", "checks_hungry", "root_busy_ns",
+                 "last_root_ns", "max_task_ns"]
+        return {k: int(v) for k, v in zip(names, out)}
+
     def stream(self) -> int:
         """cudaStream_t of the engine (for CUDA events on the launching stream)."""
         return int(self.lib.csm_gpu_stream(self.h) or 0)
