@@ -162,6 +162,23 @@ int csm_gpu_submit(csm_ctx* ctx, uint64_t n, const csm_update* ups);
  * CSM_ST_INVALID (submit vertex updates from host memory). */
 int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups);
 
+/* Counts, for each of n edges (v1, v2, label) given in device memory (n <=
+ * 1024; csm_update records with type 'e'), the embeddings of the query that
+ * contain the edge in the context's current graph -- the count an insertion
+ * of an edge already in the graph reports -- into d_counts[i] (device
+ * memory, capped at max_results; 0 for an edge with an unknown endpoint).
+ * The graph is not modified.  This entry point has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory where
+ * they need counts (a locked or stream-ordered memory pool, a latency-
+ * critical loop in which an allocation would synchronise the device): it
+ * calls no cudaMalloc, cudaFree or allocating library routine, and keeps its
+ * working memory in one static device array of 8 MiB per GPU, held while the
+ * library is loaded.  The first call on a device resolves that array and
+ * initialises it, and should come before any stream capture.  Calls share
+ * the array, so calls whose work overlaps on the GPU race.  Runs on the
+ * context's stream and waits for it. */
+int csm_gpu_probe_noalloc(csm_ctx* ctx, uint32_t n, const csm_update* d_edges, uint64_t* d_counts);
+
 /* The CUDA stream (cudaStream_t) every launch of this context is issued on,
  * so callers can time work with events on the launching stream. */
 void* csm_gpu_stream(csm_ctx* ctx);

@@ -97,6 +97,7 @@ _SIGNATURES = [
     ("csm_gpu_results", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p]),
     ("csm_gpu_results_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     ("csm_gpu_stats", C.c_int, [C.c_void_p, C.POINTER(CsmStats)]),
+    ("csm_gpu_probe_noalloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("csm_gpu_stream", C.c_void_p, [C.c_void_p]),
     ("csm_gpu_search_counters", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("csm_gpu_kernel_launches", C.c_uint64, [C.c_void_p]),

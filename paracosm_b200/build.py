@@ -32,7 +32,7 @@ CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", CXX] + ARCH
 
-CU_SOURCES = ["csm_api.cu", "csm_kernels.cu", "csm_search.cu", "csm_index.cu"]
+CU_SOURCES = ["csm_api.cu", "csm_kernels.cu", "csm_search.cu", "csm_index.cu", "csm_noalloc.cu"]
 HEADERS = [CSRC / h for h in ("csm_internal.cuh", "csm_kernels.cuh", "csm_index.cuh", "csm_host.cuh")] + [
     ROOT / "include" / "csm_gpu.h"
 ]

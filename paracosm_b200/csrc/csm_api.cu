@@ -912,3 +912,48 @@ void csm_gpu_destroy(csm_ctx* ctx) {
 }
 
 }  // extern "C"
+
+namespace csm {
+
+// Read-only device view of a context, for entry points defined in other
+// translation units.
+struct CtxView {
+  DevGraph g;
+  const Plan* plan;
+  const uint64_t* d2;
+  uint64_t d2_words;
+  uint32_t nq, n_anchor;
+  int sm_count, device;
+  cudaStream_t st;
+  uint64_t cap;
+  int homo, want_hash;
+  uint32_t warps, bps;
+};
+
+bool ctx_view(csm_ctx* ctx, CtxView* v) {
+  if (!ctx || !v || !ctx->has_graph || !ctx->has_plan) return false;
+  v->g = ctx->g;
+  v->plan = ctx->d_plan;
+  v->d2 = ctx->index.d2;
+  v->d2_words = ctx->index.words;
+  v->nq = ctx->nq;
+  v->n_anchor = ctx->h_plan->n_anchor;
+  v->sm_count = ctx->sm_count;
+  v->device = ctx->dev;
+  v->st = ctx->st;
+  v->cap = ctx->cfg.max_results;
+  v->homo = ctx->cfg.homomorphism;
+  v->want_hash = ctx->cfg.want_hash;
+  uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
+  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
+  uint32_t bps = ctx->cfg.blocks_per_sm;
+  if (!bps) {
+    const size_t smem = search_smem_bytes(ctx->nq, warps);
+    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
+  }
+  v->warps = warps;
+  v->bps = bps;
+  return true;
+}
+
+}  // namespace csm
