@@ -136,75 +136,98 @@ def get_workload(cfg: dict, n_updates: int):
     return w
 
 
-def ref_sample(w, algo: str, threads: int, cap: int, budget_s: float, hard_timeout: float):
-    """Times the reference (oracle/_ref, built from the reference sources) on a bounded
-    prefix of the stream.  The driver's watchdog ends the run after `budget_s` seconds
-    of incremental matching even inside an update (parallel TurboFlux ignores the
-    result cap below depth 2), so value = updates completed / incremental seconds."""
+def ref_start(w, algo: str, threads: int, cap: int, budget_s: float):
+    """Starts the reference (oracle/_ref, built from the reference sources) on the stream.
+    Its watchdog ends the run after `budget_s` seconds of incremental matching even
+    inside an update (parallel TurboFlux ignores the result cap below depth 2)."""
     drv = ROOT / "oracle" / "_ref" / "ref_driver"
     if not drv.exists():
-        return None, "reference driver not built (oracle/_ref/ref_driver)"
+        return None
     out = Path(tempfile.mkdtemp()) / "ref.csv"
     cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(w.directory / "data.bin"), "-U",
            str(w.directory / "stream.bin"), "-a", algo, "-t", str(threads), "--wall-budget", str(budget_s),
            "--out", str(out)]
     if cap:
         cmd += ["--max-results", str(cap)]
-    t0 = time.perf_counter()
+    p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    return {"proc": p, "out": out, "algo": algo, "threads": threads, "budget": budget_s, "t0": time.perf_counter()}
+
+
+def ref_collect(h, hard_timeout: float):
+    """value = updates completed / seconds of incremental matching, plus latency percentiles."""
+    if h is None:
+        return None, "reference driver not built (oracle/_ref/ref_driver)"
     try:
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=hard_timeout)
+        stdout, stderr = h["proc"].communicate(timeout=hard_timeout)
     except subprocess.TimeoutExpired:
+        h["proc"].kill()
         return None, f"reference driver did not finish within {hard_timeout:.0f}s"
-    wall = time.perf_counter() - t0
     done, elapsed, note = None, None, ""
-    for line in r.stdout.splitlines():
+    for line in stdout.splitlines():
         if "updates_done=" in line:
             kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
             done, elapsed = int(kv["updates_done"]), float(kv["elapsed_s"])
             if line.startswith("wall_budget_reached"):
                 note = "(budget reached inside an update)"
     if done is None:
-        return None, f"reference driver failed (exit {r.returncode}): {r.stderr[-300:]}"
+        return None, f"reference driver failed (exit {h['proc'].returncode}): {stderr[-300:]}"
     lat = []
-    if out.exists():
-        for line in out.read_text().splitlines()[1:]:
+    if h["out"].exists():
+        for line in h["out"].read_text().splitlines()[1:]:
             parts = line.split(",")
             if len(parts) >= 10:
                 lat.append(int(parts[8]))
     lat = np.array(lat, dtype=np.float64)
     if done == 0 or elapsed <= 0:
-        return None, f"no update finished within {budget_s:.0f}s {note}".strip()
+        return None, f"no update finished within {h['budget']:.0f}s {note}".strip()
     return {"updates": int(done), "seconds": elapsed, "value": done / elapsed,
             "p50_ns": float(np.percentile(lat, 50)) if len(lat) else None,
-            "p99_ns": float(np.percentile(lat, 99)) if len(lat) else None, "wall_s": wall, "note": note}, None
+            "p99_ns": float(np.percentile(lat, 99)) if len(lat) else None,
+            "wall_s": time.perf_counter() - h["t0"], "note": note, "algo": h["algo"], "threads": h["threads"]}, None
+
+
+def cpu_lines(w, cfg, budget: float) -> tuple[dict, dict]:
+    """The reference on the host cores: parallel_turboflux on all cores but one (the
+    baseline the targets are stated against) and, on the remaining core, sequential
+    SymBi, which stops at exactly --max-results like the engine does.  Both run at
+    the same time over the same stream prefix."""
+    ncpu = os.cpu_count() or 2
+    ht = ref_start(w, "parallel_turboflux", max(1, ncpu - 1), cfg["max_results"], budget)
+    hs = ref_start(w, "symbi", 1, cfg["max_results"], budget)
+    out = []
+    for h in (ht, hs):
+        r, err = ref_collect(h, budget + 900)
+        if r is None:
+            out.append({"value": None, "unit": "updates/s", "cores": h["threads"] if h else 0, "kind": "reference",
+                        "sample": err})
+        else:
+            out.append({"value": r["value"], "unit": "updates/s", "cores": r["threads"], "kind": "reference",
+                        "sample": f"first {r['updates']} updates of the same stream in {r['seconds']:.1f}s of "
+                                  f"incremental matching, {r['algo']} -t {r['threads']} (reference sources, "
+                                  f"sequential update order), {budget:.0f}s budget {r['note']}".strip(),
+                        "p50_us": (r["p50_ns"] or 0) / 1e3, "p99_us": (r["p99_ns"] or 0) / 1e3})
+    return out[0], out[1]
 
 
 def run_reference_arm(args, cfg):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    steps_upd = 64  # one reference step = 64 stream updates
     n_updates = max(cfg["min_updates"], (args.warmup + args.steps + 4) * cfg["batch"])
     w = get_workload(cfg, n_updates)
-    threads = os.cpu_count() or 1
     budget = float(os.environ.get("CSM_REF_BUDGET_S", "60"))
-    res, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], budget, budget + 900)
+    tf, sy = cpu_lines(w, cfg, budget)
     line = {"impl": "reference", "metric": METRIC, "unit": "updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "dtype": "u32", "data": "synthetic", "config": {"workload": cfg["workload"]}}
-    if res is None:
-        line.update({"value": None, "unavailable": err})
+    if tf["value"] is None:
+        line.update({"value": None, "unavailable": tf["sample"]})
     else:
-        line.update({"value": res["value"], "ms_per_step": 1000.0 * steps_upd / res["value"],
-                     "p50_us": (res["p50_ns"] or 0) / 1e3, "p99_us": (res["p99_ns"] or 0) / 1e3,
-                     "cpu_baseline": {"value": res["value"], "unit": "updates/s", "cores": threads,
-                                      "kind": "reference",
-                                      "sample": f"first {res['updates']} updates of the stream in "
-                                                f"{res['seconds']:.1f}s of incremental matching, "
-                                                f"parallel_turboflux -t {threads}, {budget:.0f}s budget "
-                                                f"{res['note']}".strip()},
-                     "e2e": {"value": res["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
+        line.update({"value": tf["value"], "ms_per_step": 1000.0 / tf["value"], "p50_us": tf.get("p50_us"),
+                     "p99_us": tf.get("p99_us"), "cpu_baseline": tf,
+                     "e2e": {"value": tf["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
                              "d2h_bytes_per_step": 0}})
+    line["sequential_symbi_capped"] = sy
     print(json.dumps(line), flush=True)
 
 
@@ -343,19 +366,9 @@ def main():
         beng.close()
 
     # ---- CPU baseline: the reference compiled from its sources, bounded sample ----
-    cpu = None
+    cpu, cpu_seq = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        r, err = ref_sample(w, "parallel_turboflux", threads, cfg["max_results"], args.cpu_budget,
-                            args.cpu_budget + 900)
-        if r is not None:
-            cpu = {"value": r["value"], "unit": "updates/s", "cores": threads, "kind": "reference",
-                   "sample": f"first {r['updates']} updates of the same stream, parallel_turboflux -t {threads} "
-                             f"(reference sources, sequential update order), {args.cpu_budget:.0f}s budget "
-                             f"{r['note']}".strip(),
-                   "p50_us": (r["p50_ns"] or 0) / 1e3, "p99_us": (r["p99_ns"] or 0) / 1e3}
-        else:
-            cpu = {"value": None, "unit": "updates/s", "cores": threads, "kind": "reference", "sample": err}
+        cpu, cpu_seq = cpu_lines(w, cfg, args.cpu_budget)
 
     if rank == 0:
         clocks = clk.summary()
@@ -375,6 +388,7 @@ def main():
                          "peak_kind": peak_kind, "kernel": "k_search", "launches": search_n,
                          "kernel_ms": search_ms, "algorithmic_bytes": work},
             "cpu_baseline": cpu,
+            "cpu_baseline_sequential_symbi_capped": cpu_seq,
             "gpu_launches": launches,
             "clocks": clocks,
             "counts": {"positive": int(res["pos"].sum()), "negative": int(res["neg"].sum()),
