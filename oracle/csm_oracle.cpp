@@ -412,3 +412,203 @@ extern "C" int oracle_brute_count(uint32_t n_qv, const uint32_t* q_vlabels, uint
   *count = c; *hash = h;
   return 0;
 }
+
+// ---- candidate index of the TurboFlux / SymBi plugins --------------------
+namespace {
+
+// Root choice shared by both plugins (ParaCOSM/CSM/matching/SymBi/symbi.cpp:113-195,
+// TurboFlux/turboflux.cpp:69-149): per query edge (u < u', in adjacency
+// order) the number of directed data entries v -> v' with L(v) = L(u),
+// L(v') = L(u') and the edge's label; the first least-frequent edge gives
+// the candidates, the endpoint whose label is rarer in the data graph wins,
+// ties go to the larger query degree (then the second endpoint).
+uint32_t dag_root(const QueryGraph& q, const Graph& g, std::vector<std::vector<uint64_t>>& freq) {
+  freq.assign(q.n, std::vector<uint64_t>(q.n, 0));
+  uint64_t min_freq = ~0ULL;
+  uint32_t mv0 = 0, mv1 = 0;
+  for (uint32_t u = 0; u < q.n; u++)
+    for (size_t i = 0; i < q.nbr[u].size(); i++) {
+      const uint32_t uo = q.nbr[u][i], lo = q.elab[u][i];
+      if (u > uo) { freq[u][uo] = freq[uo][u]; continue; }
+      uint64_t f = 0;
+      for (uint32_t v = 0; v < g.vlabel.size(); v++) {
+        if (g.vlabel[v] == NOT_EXIST || g.vlabel[v] != q.vlabel[u]) continue;
+        for (size_t j = 0; j < g.nbr[v].size(); j++)
+          if (g.label(g.nbr[v][j]) == q.vlabel[uo] && g.elab[v][j] == lo) f++;
+      }
+      freq[u][uo] = f;
+      if (f < min_freq) { min_freq = f; mv0 = u; mv1 = uo; }
+    }
+  uint64_t c0 = 0, c1 = 0;
+  for (uint32_t v = 0; v < g.vlabel.size(); v++) {
+    if (g.vlabel[v] == NOT_EXIST) continue;
+    if (g.vlabel[v] == q.vlabel[mv0]) c0++;
+    if (g.vlabel[v] == q.vlabel[mv1]) c1++;
+  }
+  if (c0 > c1) return mv1;
+  if (c0 < c1) return mv0;
+  return q.deg(mv0) > q.deg(mv1) ? mv0 : mv1;
+}
+
+struct Dag {
+  uint32_t root = 0;
+  std::vector<uint32_t> order;                 // serialized tree
+  std::vector<std::vector<uint32_t>> par, chd;  // DAG parents / children with edge labels below
+  std::vector<std::vector<uint32_t>> par_l, chd_l;
+};
+
+// SymBi (symbi.cpp:197-238): BFS from the root over all query edges; an edge
+// points from the endpoint dequeued first to the other one.
+void dag_symbi(const QueryGraph& q, uint32_t root, Dag& d) {
+  d.root = root;
+  d.order.clear();
+  d.par.assign(q.n, {}); d.chd.assign(q.n, {}); d.par_l.assign(q.n, {}); d.chd_l.assign(q.n, {});
+  std::vector<char> seen(q.n, 0), popped(q.n, 0);
+  std::vector<uint32_t> fifo{root};
+  seen[root] = 1;
+  d.order.push_back(root);
+  for (size_t h = 0; h < fifo.size(); h++) {
+    const uint32_t u = fifo[h];
+    popped[u] = 1;
+    for (size_t i = 0; i < q.nbr[u].size(); i++) {
+      const uint32_t w = q.nbr[u][i];
+      if (!seen[w]) { seen[w] = 1; fifo.push_back(w); d.order.push_back(w); }
+      if (!popped[w]) {
+        d.chd[u].push_back(w); d.chd_l[u].push_back(q.elab[u][i]);
+        d.par[w].push_back(u); d.par_l[w].push_back(q.elab[u][i]);
+      }
+    }
+  }
+}
+
+// TurboFlux (turboflux.cpp:151-219): a spanning tree grown level by level;
+// inside a level the cheapest pending edge (first of equal frequency) is
+// taken and every other pending edge into the same vertex is dropped.  The
+// serialized tree is the BFS order over tree children.
+void dag_turboflux(const QueryGraph& q, uint32_t root, const std::vector<std::vector<uint64_t>>& freq, Dag& d) {
+  d.root = root;
+  d.par.assign(q.n, {}); d.chd.assign(q.n, {}); d.par_l.assign(q.n, {}); d.chd_l.assign(q.n, {});
+  struct EF { uint32_t a, b; uint64_t f; };
+  std::vector<char> vis(q.n, 0);
+  vis[root] = 1;
+  std::vector<EF> cur;
+  for (uint32_t w : q.nbr[root]) cur.push_back({root, w, freq[root][w]});
+  while (!cur.empty()) {
+    std::vector<EF> next;
+    while (!cur.empty()) {
+      size_t best = 0;
+      for (size_t i = 1; i < cur.size(); i++) if (cur[i].f < cur[best].f) best = i;
+      const EF m = cur[best];
+      std::vector<EF> keep;
+      for (const EF& e : cur) if (e.b != m.b) keep.push_back(e);
+      cur.swap(keep);
+      if (vis[m.b]) continue;
+      vis[m.b] = 1;
+      const uint32_t l = q.edge_label(m.a, m.b);
+      d.chd[m.a].push_back(m.b); d.chd_l[m.a].push_back(l);
+      d.par[m.b].push_back(m.a); d.par_l[m.b].push_back(l);
+      for (uint32_t w : q.nbr[m.b]) if (!vis[w]) next.push_back({m.b, w, freq[m.b][w]});
+    }
+    cur.swap(next);
+  }
+  d.order.clear();
+  std::vector<uint32_t> fifo{root};
+  for (size_t h = 0; h < fifo.size(); h++) {
+    d.order.push_back(fifo[h]);
+    for (uint32_t w : d.chd[fifo[h]]) fifo.push_back(w);
+  }
+}
+
+bool has_support(const Graph& g, uint32_t v, uint32_t lab, uint32_t el, const std::vector<char>& flag) {
+  for (size_t j = 0; j < g.nbr[v].size(); j++) {
+    const uint32_t w = g.nbr[v][j];
+    if (g.elab[v][j] == el && g.label(w) == lab && flag[w]) return true;
+  }
+  return false;
+}
+
+// d1 / d2 flags by their definition (symbi.cpp:259-349; the counters n1,
+// np1, n2, nc2 of InsertionTopDown ... DeletionBottomUp, symbi.cpp:404-469,
+// maintain the same fixpoint under updates):
+//   d1[u][v]: L(v) = L(u) and every DAG parent p has a neighbour w of v over
+//             an edge labelled l(u, p) with d1[p][w];
+//   d2[u][v]: d1[u][v] and every DAG child c has a neighbour w of v over an
+//             edge labelled l(u, c) with d2[c][w].
+void dag_flags(const QueryGraph& q, const Graph& g, const Dag& d, std::vector<std::vector<char>>& d1,
+               std::vector<std::vector<char>>& d2) {
+  const size_t n = g.vlabel.size();
+  d1.assign(q.n, std::vector<char>(n, 0));
+  d2.assign(q.n, std::vector<char>(n, 0));
+  for (uint32_t u : d.order)
+    for (uint32_t v = 0; v < n; v++) {
+      if (g.vlabel[v] == NOT_EXIST || g.vlabel[v] != q.vlabel[u]) continue;
+      bool ok = true;
+      for (size_t k = 0; k < d.par[u].size() && ok; k++)
+        ok = has_support(g, v, q.vlabel[d.par[u][k]], d.par_l[u][k], d1[d.par[u][k]]);
+      d1[u][v] = ok;
+    }
+  for (size_t i = d.order.size(); i-- > 0;) {
+    const uint32_t u = d.order[i];
+    for (uint32_t v = 0; v < n; v++) {
+      if (!d1[u][v]) continue;
+      bool ok = true;
+      for (size_t k = 0; k < d.chd[u].size() && ok; k++)
+        ok = has_support(g, v, q.vlabel[d.chd[u][k]], d.chd_l[u][k], d2[d.chd[u][k]]);
+      d2[u][v] = ok;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                            uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                            uint64_t n_up, const oracle_update* ups, int algo, uint32_t* root, uint32_t* order,
+                            uint32_t* parents, uint64_t words, uint64_t* d1_out, uint64_t* d2_out) {
+  QueryGraph q;
+  if (n_qv < 2 || n_qv > 32 || !q.build(n_qv, q_vlabels, n_qe, q_edges) || q.n_edges == 0) return -1;
+  if (algo != ORACLE_INDEX_TURBOFLUX && algo != ORACLE_INDEX_SYMBI) return -2;
+  Graph g;
+  for (uint32_t v = 0; v < n_v; v++) g.add_vertex(v, vlabels[v]);
+  if (g.vlabel.size() < n_v) { g.vlabel.resize(n_v, NOT_EXIST); g.nbr.resize(n_v); g.elab.resize(n_v); }
+  for (uint64_t i = 0; i < n_e; i++) {
+    uint32_t a = edges[3 * i], b = edges[3 * i + 1];
+    if (a < n_v && b < n_v && a != b) g.add_edge(a, b, edges[3 * i + 2]);
+  }
+  // the DAG is fixed at preprocessing, on the graph before the stream
+  std::vector<std::vector<uint64_t>> freq;
+  const uint32_t r = dag_root(q, g, freq);
+  Dag d;
+  if (algo == ORACLE_INDEX_SYMBI) dag_symbi(q, r, d); else dag_turboflux(q, r, freq, d);
+  for (uint64_t i = 0; i < n_up; i++) {  // the graph after the stream prefix
+    const oracle_update& u = ups[i];
+    if (u.type == 'v') {
+      if (u.is_add) g.add_vertex(u.id1, u.label);
+      else if (u.id1 < g.vlabel.size()) {
+        std::vector<uint32_t> ns = g.nbr[u.id1];
+        for (uint32_t w : ns) g.remove_edge(u.id1, w);
+        g.vlabel[u.id1] = NOT_EXIST;
+      }
+      continue;
+    }
+    if (u.id1 >= g.vlabel.size() || u.id2 >= g.vlabel.size() || u.id1 == u.id2) continue;
+    if (u.is_add) g.add_edge(u.id1, u.id2, u.label); else g.remove_edge(u.id1, u.id2);
+  }
+  const size_t n = g.vlabel.size();
+  if (words * 64 < n) return -3;
+  std::vector<std::vector<char>> d1, d2;
+  dag_flags(q, g, d, d1, d2);
+  *root = d.root;
+  for (uint32_t i = 0; i < n_qv; i++) order[i] = d.order[i];
+  for (uint32_t u = 0; u < n_qv; u++) {
+    uint32_t m = 0;
+    for (uint32_t p : d.par[u]) m |= 1u << p;
+    parents[u] = m;
+    for (uint64_t w = 0; w < words; w++) { d1_out[u * words + w] = 0; d2_out[u * words + w] = 0; }
+    for (size_t v = 0; v < n; v++) {
+      if (d1[u][v]) d1_out[u * words + (v >> 6)] |= 1ULL << (v & 63);
+      if (d2[u][v]) d2_out[u * words + (v >> 6)] |= 1ULL << (v & 63);
+    }
+  }
+  return (int)n;
+}

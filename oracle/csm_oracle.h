@@ -13,6 +13,9 @@
  *   - deletion: count before removing ... matching/GraphFlow/graphflow.cpp:357-416
  *   - per-update result cap ............. matching/SymBi/symbi.cpp:583 (stop at exactly the cap)
  *   - label-triple safe test ............ matching/Parallel_GraphFlow/parallel_graphflow.cpp:1990-2016
+ *   - DAG root / SymBi DAG .............. matching/SymBi/symbi.cpp:113-238
+ *   - TurboFlux spanning tree ........... matching/TurboFlux/turboflux.cpp:69-219
+ *   - d1 / d2 candidate flags ........... matching/SymBi/symbi.cpp:259-349, 404-469
  *
  * Counts are the number of injective (unless homomorphism), label-preserving
  * embeddings of the query that contain the updated edge.  The match-set hash
@@ -65,6 +68,20 @@ int oracle_brute_count(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, 
  * is the j-th query vertex of the order anchored on the i-th query edge. */
 int oracle_graphflow_orders(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
                             uint32_t* order);
+
+/* Candidate index (the d1 / d2 flags) of the TurboFlux plugin (a DCG over a
+ * query spanning tree, ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:69-331)
+ * or the SymBi plugin (a DCS over a DAG of every query edge,
+ * SymBi/symbi.cpp:113-349).  The DAG is chosen on the graph before the
+ * stream; the flags are those of the graph after the first n_up updates.
+ * Outputs: root, order[n_qv] (serialized tree), parents[n_qv] (bitmask of DAG
+ * parents), d1 / d2 as [n_qv][words] bitsets over data vertex ids.  Returns
+ * the number of data vertex ids, or a negative value on bad input. */
+enum { ORACLE_INDEX_TURBOFLUX = 1, ORACLE_INDEX_SYMBI = 2 };
+int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                 uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                 uint64_t n_up, const oracle_update* ups, int algo, uint32_t* root, uint32_t* order,
+                 uint32_t* parents, uint64_t words, uint64_t* d1, uint64_t* d2);
 
 #ifdef __cplusplus
 }

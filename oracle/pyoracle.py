@@ -43,6 +43,11 @@ def lib() -> C.CDLL:
                                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         _lib.oracle_graphflow_orders.restype = C.c_int
         _lib.oracle_graphflow_orders.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        _lib.oracle_index.restype = C.c_int
+        _lib.oracle_index.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                      C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
+                                      C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                      C.c_void_p]
     return _lib
 
 
@@ -87,6 +92,84 @@ def graphflow_orders(q_vlabels, q_edges) -> np.ndarray:
     if m < 0:
         raise RuntimeError("bad query")
     return out[:m]
+
+
+INDEX_ALGOS = {"turboflux": 1, "symbi": 2, "parallel_turboflux": 1, "parallel_symbi": 2}
+
+
+def index(q_vlabels, q_edges, vlabels, edges, updates=None, *, algo: str = "symbi") -> dict:
+    """Candidate index of the TurboFlux / SymBi plugin after the given updates.
+
+    Returns root, order (serialized tree), parents (sorted lists per query
+    vertex) and d1 / d2 as bool arrays of shape [n_qv, n_vertices].
+    """
+    qv = np.ascontiguousarray(q_vlabels, dtype=np.uint32)
+    qe = np.ascontiguousarray(q_edges, dtype=np.uint32).reshape(-1, 3)
+    vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+    e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
+    u = np.ascontiguousarray(updates if updates is not None else np.zeros(0, UPDATE_DTYPE), dtype=UPDATE_DTYPE)
+    nmax = len(vl)
+    for r in u:
+        if r["type"] == ord("v"):
+            nmax = max(nmax, int(r["id1"]) + 1)
+    words = (nmax + 63) // 64 + 1
+    root = C.c_uint32()
+    order = np.zeros(len(qv), dtype=np.uint32)
+    parents = np.zeros(len(qv), dtype=np.uint32)
+    d1 = np.zeros((len(qv), words), dtype=np.uint64)
+    d2 = np.zeros((len(qv), words), dtype=np.uint64)
+    n = lib().oracle_index(len(qv), _p(qv), len(qe), _p(qe), len(vl), _p(vl), len(e), _p(e), len(u), _p(u),
+                           INDEX_ALGOS[algo], C.byref(root), _p(order), _p(parents), words, _p(d1), _p(d2))
+    if n < 0:
+        raise RuntimeError(f"oracle_index failed: {n}")
+    bits = lambda a: np.unpackbits(a.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)  # noqa: E731
+    par = [[p for p in range(len(qv)) if (int(parents[q]) >> p) & 1] for q in range(len(qv))]
+    return {"root": int(root.value), "order": order.tolist(), "parents": par, "d1": bits(d1), "d2": bits(d2)}
+
+
+def parse_index_dump(text: str, n_vertices: int) -> dict:
+    """Parses ref_driver --dump-index output into {at: index dict} (same keys as index())."""
+    out: dict = {}
+    cur = None
+    for line in text.splitlines():
+        t = line.split()
+        if not t:
+            continue
+        if t[0] == "at":
+            cur = {"parents": {}, "d1": {}, "d2": {}}
+            out[int(t[1])] = cur
+        elif t[0] == "root":
+            cur["root"] = int(t[1])
+        elif t[0] == "order":
+            cur["order"] = [int(x) for x in t[1:]]
+        elif t[0] == "parents":
+            cur["parents"][int(t[1])] = sorted(int(x) for x in t[2:])
+        elif t[0] in ("d1", "d2"):
+            cur[t[0]][int(t[1])] = [int(x) for x in t[2:]]
+    for cur in out.values():
+        nq = len(cur["order"])
+        cur["parents"] = [cur["parents"][q] for q in range(nq)]
+        for k in ("d1", "d2"):
+            a = np.zeros((nq, n_vertices), dtype=bool)
+            for q, vs in cur[k].items():
+                a[q, vs] = True
+            cur[k] = a
+    return out
+
+
+def ref_index(query, data, stream, algo: str, at: list[int], n_vertices: int, *, timeout: float = 600) -> dict:
+    """The reference plugin's own index state after each update count in `at` (0: after preprocessing)."""
+    if not REF_DRIVER.exists():
+        raise RuntimeError(f"reference driver not built: {REF_DRIVER}")
+    tmp = Path(os.environ.get("TMPDIR", "/tmp")) / f"refidx_{os.getpid()}_{algo}.txt"
+    cmd = [str(REF_DRIVER), "-q", str(query), "-d", str(data), "-u", str(stream), "-a", algo, "--dump-index",
+           str(tmp), "--dump-at", ",".join(str(x) for x in at)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
+    text = tmp.read_text()
+    tmp.unlink(missing_ok=True)
+    return parse_index_dump(text, n_vertices)
 
 
 def ref_run(query: str | os.PathLike, data: str | os.PathLike, stream: str | os.PathLike, algo: str, *,

@@ -49,6 +49,9 @@
 #include "utils/globals.h"
 #include "utils/types.h"
 
+// ref_index_access.cpp: the sequential SymBi / TurboFlux index state
+bool ref_dump_index(matching* m, const std::string& algo, uint32_t nq, FILE* f, long at);
+
 namespace {
 
 // MurmurHash3 fmix64 finaliser (public domain).
@@ -100,7 +103,8 @@ class EnumHashBuf : public std::streambuf {
 };
 
 struct Args {
-  std::string q, d, u, algo = "graphflow", out, dbin, ubin;
+  std::string q, d, u, algo = "graphflow", out, dbin, ubin, dump_index;
+  std::vector<long> dump_at;  // update counts after which the index is dumped (0: after preprocessing)
   size_t threads = 1, auto_tuning = 0, max_updates = SIZE_MAX;
   uint64_t max_results = UINT32_MAX;
   double time_budget = 0;   // stop after the update that crosses this many seconds
@@ -158,7 +162,8 @@ void usage() {
   fprintf(stderr,
           "ref_driver -q query -d data|-D data.bin -u stream|-U stream.bin -a algo\n"
           "  [-t threads] [--auto-tuning 0|1] [--max-results N] [--homo 0|1]\n"
-          "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S] [--wall-budget S]\n");
+          "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S] [--wall-budget S]\n"
+          "  [--dump-index FILE --dump-at N,N,...]   (symbi / turboflux: root, DAG, d1 / d2 flags)\n");
 }
 
 }  // namespace
@@ -183,6 +188,12 @@ int main(int argc, char** argv) {
     else if (k == "--max-updates") a.max_updates = std::stoull(nxt());
     else if (k == "--time-budget") a.time_budget = std::stod(nxt());
     else if (k == "--wall-budget") a.wall_budget = std::stod(nxt());
+    else if (k == "--dump-index") a.dump_index = nxt();
+    else if (k == "--dump-at") {
+      std::stringstream ss(nxt());
+      std::string t;
+      while (std::getline(ss, t, ',')) if (!t.empty()) a.dump_at.push_back(std::stol(t));
+    }
     else { usage(); return 2; }
   }
   if (a.q.empty() || (a.d.empty() && a.dbin.empty()) || (a.u.empty() && a.ubin.empty())) { usage(); return 2; }
@@ -222,6 +233,16 @@ int main(int argc, char** argv) {
     if (!fo) { fprintf(stderr, "cannot write %s\n", a.out.c_str()); return 1; }
     fprintf(fo, "idx,type,is_add,id1,id2,label,pos,neg,latency_ns,hash\n");
   }
+  FILE* fdump = nullptr;
+  if (!a.dump_index.empty()) {
+    fdump = fopen(a.dump_index.c_str(), "w");
+    if (!fdump) { fprintf(stderr, "cannot write %s\n", a.dump_index.c_str()); return 1; }
+  }
+  auto want_dump = [&](long at) { return fdump && std::find(a.dump_at.begin(), a.dump_at.end(), at) != a.dump_at.end(); };
+  if (want_dump(0) && !ref_dump_index(mm, a.algo, query.NumVertices(), fdump, 0)) {
+    fprintf(stderr, "--dump-index supports symbi and turboflux\n");
+    return 2;
+  }
   if (a.hash) old = std::cout.rdbuf(&hb);
 
   size_t pos_last = 0, neg_last = 0, unsafe = 0, nv = 0, ne = 0, done = 0;
@@ -258,6 +279,7 @@ int main(int argc, char** argv) {
     if (pc != pos_last || nc != neg_last) unsafe++;
     pos_last = pc; neg_last = nc;
     done++;
+    if (want_dump((long)done)) { ref_dump_index(mm, a.algo, query.NumVertices(), fdump, (long)done); fflush(fdump); }
     g_done.store(done);
     if (a.time_budget > 0 &&
         std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count() > a.time_budget)
@@ -266,6 +288,7 @@ int main(int argc, char** argv) {
   auto te = std::chrono::steady_clock::now();
   if (a.hash) std::cout.rdbuf(old);
   if (fo) fclose(fo);
+  if (fdump) fclose(fdump);
 
   std::vector<uint64_t> l(lat.begin(), lat.begin() + done);
   std::sort(l.begin(), l.end());

@@ -39,6 +39,33 @@ def load_golden(name: str) -> dict:
     return {"dir": d, "params": params, "qv": qv, "qe": qe, "vl": vl, "e": e, "stream": s, "exp": exp}
 
 
+def load_golden_index(name: str, algo: str) -> dict:
+    """The reference plugin's own index state ({update count: {root, order, parents, d1, d2}}),
+    with d1 / d2 as bool arrays [n_qv, n_vertices]."""
+    d = GOLDEN / name
+    n = len(load_golden(name)["vl"])
+    out: dict = {}
+    cur = None
+    for line in (d / f"index_{algo}.txt").read_text().splitlines():
+        t = line.split()
+        if t[0] == "at":
+            cur = {"parents": [], "d1": [], "d2": []}
+            out[int(t[1])] = cur
+        elif t[0] == "root":
+            cur["root"] = int(t[1])
+        elif t[0] == "order":
+            cur["order"] = [int(x) for x in t[1:]]
+        elif t[0] == "parents":
+            cur["parents"].append([int(x) for x in t[2:]])
+        else:
+            bits = np.unpackbits(np.frombuffer(bytes.fromhex(t[2]), dtype=np.uint8), bitorder="little")
+            cur[t[0]].append(bits[:n].astype(bool))
+    for cur in out.values():
+        cur["d1"] = np.array(cur["d1"])
+        cur["d2"] = np.array(cur["d2"])
+    return out
+
+
 @pytest.fixture(scope="session")
 def gen_dir(tmp_path_factory):
     return tmp_path_factory.mktemp("workloads")

@@ -6,9 +6,14 @@ run through the reference plugins compiled from their sources
 sequential per-update semantics of the reference's SingleThreadUpdate loop.
 The fixture keeps the inputs in the reference's text formats and, per
 update, the positive / negative counts of each plugin and the match-set hash
-of sequential SymBi (parsed from its --print-enum output).
+of sequential SymBi (parsed from its --print-enum output).  index_symbi.txt
+and index_turboflux.txt hold those plugins' own candidate index (root,
+serialized DAG, parents, d1 / d2 flags as little-endian hex bitsets) after
+preprocessing, after half of the stream and after all of it, read out of the
+plugin objects by ref_driver --dump-index.
 
     python tests/golden/make_golden.py          # needs the reference sources to build the driver
+    python tests/golden/make_golden.py --index  # only the index fixtures
 
 Only this script reads the reference; the fixtures it writes are plain files.
 """
@@ -53,7 +58,32 @@ PLUGINS = [("graphflow", 1), ("symbi", 1), ("turboflux", 1), ("parallel_graphflo
            ("parallel_symbi", 32)]
 
 
+def write_index(d: Path) -> None:
+    """Writes index_<algo>.txt for one case from the reference's own index state."""
+    import numpy as np
+
+    vl, _ = workload.read_graph(d / "data.graph")
+    n_up = len(workload.read_stream(d / "stream.txt"))
+    ats = [0, n_up // 2, n_up]
+    for algo in ("symbi", "turboflux"):
+        ref = pyoracle.ref_index(d / "query.graph", d / "data.graph", d / "stream.txt", algo, ats, len(vl))
+        with open(d / f"index_{algo}.txt", "w") as f:
+            for at in ats:
+                r = ref[at]
+                f.write(f"at {at}\nroot {r['root']}\norder {' '.join(map(str, r['order']))}\n")
+                for q, ps in enumerate(r["parents"]):
+                    f.write(f"parents {q} {' '.join(map(str, ps))}".rstrip() + "\n")
+                for k in ("d1", "d2"):
+                    for q in range(len(r["order"])):
+                        f.write(f"{k} {q} {np.packbits(r[k][q], bitorder='little').tobytes().hex()}\n")
+
+
 def main() -> None:
+    if "--index" in sys.argv:
+        for name in CASES:
+            write_index(HERE / name)
+            print(name, "index fixtures")
+        return
     for name, (args, cap, homo) in CASES.items():
         d = HERE / name
         tmp = HERE / f"_tmp_{name}"
@@ -98,6 +128,7 @@ def main() -> None:
                 f.write(",".join(row) + "\n")
         (d / "params.json").write_text(json.dumps({"max_results": cap, "homo": homo, "generator": args,
                                                    "plugins": [a for a, _ in PLUGINS if a in cols]}, indent=1))
+        write_index(d)
         print(name, "updates", n, "plugins", list(cols))
 
 

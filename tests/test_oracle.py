@@ -5,7 +5,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden
+from conftest import golden_cases, load_golden, load_golden_index
 from oracle import pyoracle
 
 UPD = pyoracle.UPDATE_DTYPE
@@ -114,3 +114,51 @@ def test_oracle_cap_stops_at_exactly_the_cap():
     tot = full["pos"] + full["neg"]
     assert np.array_equal(np.minimum(tot, 40), r["pos"] + r["neg"])
     assert np.array_equal(capped, tot >= 40)
+
+
+@pytest.mark.parametrize("algo", ["symbi", "turboflux"])
+@pytest.mark.parametrize("case", golden_cases())
+def test_oracle_index_matches_the_reference_plugins_own_index(case, algo):
+    """Root, DAG and the d1 / d2 flags, against the state read out of the reference's
+    SymBi / TurboFlux objects after preprocessing, half of the stream and all of it."""
+    g = load_golden(case)
+    ref = load_golden_index(case, algo)
+    for at, r in ref.items():
+        o = pyoracle.index(g["qv"], g["qe"], g["vl"], g["e"], g["stream"][:at], algo=algo)
+        assert o["root"] == r["root"] and o["order"] == r["order"] and o["parents"] == r["parents"]
+        n = r["d1"].shape[1]
+        assert np.array_equal(o["d1"][:, :n], r["d1"]), at
+        assert np.array_equal(o["d2"][:, :n], r["d2"]), at
+        assert not o["d1"][:, n:].any() and not o["d2"][:, n:].any()
+
+
+def test_oracle_index_is_the_fixpoint_by_definition():
+    """d1 / d2 on a tiny graph, checked against a direct evaluation of the definition."""
+    rng = np.random.default_rng(5)
+    n = 40
+    vl = rng.integers(0, 2, n).astype(np.uint32)
+    e = np.array([(a, b, int(rng.integers(0, 2))) for a in range(n) for b in range(a + 1, n) if rng.random() < 0.12],
+                 dtype=np.uint32)
+    qv = np.array([0, 1, 0, 1], dtype=np.uint32)
+    qe = np.array([(0, 1, 0), (1, 2, 1), (2, 3, 0), (0, 2, 0)], dtype=np.uint32)
+    adj = {}
+    for a, b, l in e:
+        adj.setdefault(int(a), []).append((int(b), int(l)))
+        adj.setdefault(int(b), []).append((int(a), int(l)))
+    ql = {(int(a), int(b)): int(l) for a, b, l in qe}
+    ql.update({(b, a): l for (a, b), l in ql.items()})
+    for algo in ("symbi", "turboflux"):
+        o = pyoracle.index(qv, qe, vl, e, algo=algo)
+        par = o["parents"]
+        chd = [[c for c in range(4) if u in par[c]] for u in range(4)]
+        d1 = np.zeros((4, n), bool)
+        d2 = np.zeros((4, n), bool)
+        sup = lambda v, w_lab, el, flag: any(vl[w] == w_lab and l == el and flag[w] for w, l in adj.get(v, []))  # noqa: E731
+        for u in o["order"]:
+            for v in range(n):
+                d1[u, v] = vl[v] == qv[u] and all(sup(v, qv[p], ql[(u, p)], d1[p]) for p in par[u])
+        for u in reversed(o["order"]):
+            for v in range(n):
+                d2[u, v] = d1[u, v] and all(sup(v, qv[c], ql[(u, c)], d2[c]) for c in chd[u])
+        assert np.array_equal(o["d1"], d1) and np.array_equal(o["d2"], d2)
+        assert o["order"][0] == o["root"] and par[o["root"]] == []
