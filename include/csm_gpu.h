@@ -111,7 +111,7 @@ typedef struct csm_stats {
   uint64_t device_bytes;      /* device memory held by the context */
   uint64_t pool_entries, pool_capacity;
   double last_batch_ms, total_device_ms;
-  uint64_t index_entries, index_vertices; /* GetMemoryCost analogue */
+  uint64_t index_entries, index_vertices; /* set d1 / set d2 flags over all query vertices (TurboFlux / SymBi) */
   uint64_t search_launches;   /* launches of the search kernel */
   double search_ms;           /* their summed duration, from CUDA events on the launching stream */
   uint64_t work_bytes;        /* algorithmic bytes of all completed updates (csm_result.work_bytes) */
@@ -178,6 +178,30 @@ int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups);
  * the array, so calls whose work overlaps on the GPU race.  Runs on the
  * context's stream and waits for it. */
 int csm_gpu_probe_noalloc(csm_ctx* ctx, uint32_t n, const csm_update* d_edges, uint64_t* d_counts);
+
+/* Candidate index of the TurboFlux / SymBi plugins: the DAG the index is
+ * defined over.  The reference keeps these as private plugin members
+ * (q_root_, serialized_tree_, treeNode_[u].backwards_,
+ * ParaCOSM/CSM/matching/SymBi/symbi.h:33-44); there is no reference entry
+ * point.  They back the index parity tests and debugging. */
+typedef struct csm_index_info {
+  int32_t algorithm;     /* CSM_ALGO_*; GRAPHFLOW (no index): the rest is zero */
+  uint32_t n_qv;
+  uint32_t root;         /* q_root_ */
+  uint32_t reserved;
+  uint64_t words;        /* 64-bit words per flag row */
+  uint32_t order[32];    /* serialized_tree_ (a topological order of the DAG) */
+  uint32_t parents[32];  /* bitmask of DAG parents per query vertex (treeNode_[u].backwards_) */
+  uint64_t d1_count, d2_count;  /* set flags over all query vertices */
+} csm_index_info;
+int csm_gpu_index_info(csm_ctx* ctx, csm_index_info* out);
+
+/* Copies the d1 (which = 1) or d2 (which = 2) flags (symbi.h:55-56: per
+ * query vertex, the data vertices that pass the top-down / the full filter)
+ * to host memory as [n_qv][out_words] little-endian bitsets over data vertex
+ * ids; out_words must be at least csm_index_info.words.  Waits for the
+ * context's stream.  No reference entry point (private members there). */
+int csm_gpu_index_flags(csm_ctx* ctx, uint32_t which, uint64_t* out, uint64_t out_words);
 
 /* The CUDA stream (cudaStream_t) every launch of this context is issued on,
  * so callers can time work with events on the launching stream. */

@@ -82,6 +82,14 @@ class CsmStats(C.Structure):
     ]
 
 
+class CsmIndexInfo(C.Structure):
+    _fields_ = [
+        ("algorithm", C.c_int32), ("n_qv", C.c_uint32), ("root", C.c_uint32), ("reserved", C.c_uint32),
+        ("words", C.c_uint64), ("order", C.c_uint32 * 32), ("parents", C.c_uint32 * 32),
+        ("d1_count", C.c_uint64), ("d2_count", C.c_uint64),
+    ]
+
+
 # Every symbol include/csm_gpu.h declares: (name, restype, argtypes).
 _SIGNATURES = [
     ("csm_gpu_default_cfg", None, [C.POINTER(CsmCfg)]),
@@ -98,6 +106,8 @@ _SIGNATURES = [
     ("csm_gpu_results_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     ("csm_gpu_stats", C.c_int, [C.c_void_p, C.POINTER(CsmStats)]),
     ("csm_gpu_probe_noalloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("csm_gpu_index_info", C.c_int, [C.c_void_p, C.POINTER(CsmIndexInfo)]),
+    ("csm_gpu_index_flags", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]),
     ("csm_gpu_stream", C.c_void_p, [C.c_void_p]),
     ("csm_gpu_search_counters", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("csm_gpu_kernel_launches", C.c_uint64, [C.c_void_p]),

@@ -352,7 +352,7 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
   k_mut_insert<<<mut_blocks, 256, 0, st>>>(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g); CKL();
   // candidate index: union-graph insertions
-  int rc = index_apply_insertions(ctx->index, g, ctx->d_ins2, c + 3, ctx->d_rins, st, &ctx->launches);
+  int rc = index_apply_edges(ctx->index, g, ctx->d_ins2, L, st, &ctx->launches);
   if (rc) return rc;
   // search
   k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, ctx->d_info, g, ctx->d_plan, ctx->index.d2, ctx->index.words,
@@ -390,7 +390,7 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, ctx->d_stamp, out); CKL();
   // union graph -> CSR after the batch
   k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, g); CKL();
-  rc = index_apply_deletions(ctx->index, g, ctx->d_del2, c + 4, ctx->d_rdel, st, &ctx->launches);
+  rc = index_apply_edges(ctx->index, g, ctx->d_del2, L, st, &ctx->launches);
   if (rc) return rc;
   k_temporal_clear<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
   ctx->batches++;
@@ -403,7 +403,7 @@ static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_upda
   k_vertex_update<<<1, 32, 0, st>>>(ups, 1, ctx->g, ctx->d_info); CKL();
   CK(cudaMemsetAsync(ctx->d_safe, 0xff, 4, st));
   k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, 0, 0, out); CKL();
-  int rc = index_vertex_update(ctx->index, ctx->g, ups, st, &ctx->launches);
+  int rc = index_vertex_update(ctx->index, ctx->g, h, st, &ctx->launches);
   return rc;
 }
 
@@ -766,8 +766,11 @@ int csm_gpu_build_index(csm_ctx* ctx) {
   if (rc) return rc;
   rc = ensure_batch_buffers(ctx);
   if (rc) return rc;
-  IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &ctx->qel};
-  return index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->st, &ctx->launches);
+  std::vector<std::vector<uint32_t>> qel_f(ctx->nq);
+  for (uint32_t u = 0; u < ctx->nq; u++)
+    for (uint32_t l : ctx->qel[u]) qel_f[u].push_back(fold_host(ctx->qlab_e, l));
+  IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &qel_f};
+  return index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->sm_count, ctx->st, &ctx->launches);
 }
 
 int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
@@ -864,6 +867,11 @@ int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
     CK(cudaMemcpy(&ps, ctx->g.ps, sizeof(ps), cudaMemcpyDeviceToHost));
     out->pool_entries = ps.top[ps.active];
   }
+  {
+    uint64_t d1c = 0, d2c = 0;
+    int irc = index_counts(ctx->index, ctx->st, &d1c, &d2c);
+    if (irc) return irc;
+  }
   index_stats(ctx->index, &out->index_entries, &out->index_vertices);
   out->num_edges = ctx->num_edges;
   if (ctx->d_q) {
@@ -884,6 +892,42 @@ int csm_gpu_stats(csm_ctx* ctx, csm_stats* out) {
 uint64_t csm_gpu_kernel_launches(csm_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 void* csm_gpu_stream(csm_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+
+int csm_gpu_index_info(csm_ctx* ctx, csm_index_info* out) {
+  if (!ctx || !out) return set_err(CSM_EINVAL, "null argument");
+  CK(cudaSetDevice(ctx->dev));
+  memset(out, 0, sizeof(*out));
+  out->algorithm = ctx->cfg.algorithm;
+  const IndexState& ix = ctx->index;
+  if (!ix.active) { out->algorithm = CSM_ALGO_GRAPHFLOW; return CSM_OK; }
+  out->n_qv = ix.h_dag.nq;
+  out->root = ix.root;
+  out->words = ix.words;
+  for (uint32_t i = 0; i < ix.h_dag.nq; i++) {
+    out->order[i] = ix.order[i];
+    uint32_t m = 0;
+    for (uint32_t k = 0; k < ix.h_dag.npar[i]; k++) m |= 1u << ix.h_dag.par[i][k];
+    out->parents[i] = m;
+  }
+  return index_counts(ctx->index, ctx->st, &out->d1_count, &out->d2_count);
+}
+
+int csm_gpu_index_flags(csm_ctx* ctx, uint32_t which, uint64_t* out, uint64_t out_words) {
+  if (!ctx || !out) return set_err(CSM_EINVAL, "null argument");
+  const IndexState& ix = ctx->index;
+  if (!ix.active) return set_err(CSM_ESTATE, "no candidate index (GraphFlow, or build_index not called)");
+  if (which != 1 && which != 2) return set_err(CSM_EINVAL, "which must be 1 (d1) or 2 (d2)");
+  if (out_words < ix.words) return set_err(CSM_EINVAL, "out_words below %llu", (unsigned long long)ix.words);
+  CK(cudaSetDevice(ctx->dev));
+  const uint64_t* src = which == 1 ? ix.bits.d1 : ix.bits.d2;
+  CK(cudaMemcpy2DAsync(out, 8ull * out_words, src, 8ull * ix.words, 8ull * ix.words, ix.h_dag.nq,
+                       cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (out_words > ix.words)
+    for (uint32_t u = 0; u < ix.h_dag.nq; u++)
+      memset(out + (uint64_t)u * out_words + ix.words, 0, 8ull * (out_words - ix.words));
+  return CSM_OK;
+}
 
 int csm_gpu_search_counters(csm_ctx* ctx, uint64_t* out, uint32_t n) {
   if (!ctx || (n && !out)) return set_err(CSM_EINVAL, "null argument");

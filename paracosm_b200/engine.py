@@ -22,7 +22,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (ALGORITHMS, MODE_BATCHED, MODE_PLAIN, RESULT_DTYPE, UPDATE_DTYPE, CsmCfg, CsmStats, check,
+from ._abi import (ALGORITHMS, MODE_BATCHED, MODE_PLAIN, RESULT_DTYPE, UPDATE_DTYPE, CsmCfg, CsmIndexInfo, CsmStats, check,
                    load_library)
 
 NOT_EXIST = 0xFFFFFFFF
@@ -140,6 +140,24 @@ class Engine:
         names = ["busy_ns", "idle_ns", "iters", "donations", "starved", "checks", "checks_hungry", "root_busy_ns",
                  "last_root_ns", "max_task_ns"]
         return {k: int(v) for k, v in zip(names, out)}
+
+    def index(self, n_vertices: int | None = None) -> dict | None:
+        """The TurboFlux / SymBi candidate index: root, order, parents (sorted lists) and d1 / d2
+        as bool arrays [n_qv, n_vertices]; None for GraphFlow."""
+        info = CsmIndexInfo()
+        check(self.lib, self.lib.csm_gpu_index_info(self.h, C.byref(info)))
+        if info.algorithm == 0 or info.n_qv == 0:
+            return None
+        nq, words = int(info.n_qv), int(info.words)
+        out = {"root": int(info.root), "order": [int(x) for x in info.order[:nq]],
+               "parents": [[p for p in range(nq) if (int(info.parents[u]) >> p) & 1] for u in range(nq)],
+               "d1_count": int(info.d1_count), "d2_count": int(info.d2_count)}
+        n = n_vertices if n_vertices is not None else 64 * words
+        for which, key in ((1, "d1"), (2, "d2")):
+            buf = np.zeros((nq, words), dtype=np.uint64)
+            check(self.lib, self.lib.csm_gpu_index_flags(self.h, which, _ptr(buf), words))
+            out[key] = np.unpackbits(buf.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)
+        return out
 
     def stream(self) -> int:
         """cudaStream_t of the engine (for CUDA events on the launching stream)."""

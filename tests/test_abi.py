@@ -32,15 +32,17 @@ def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include "csm_gpu.h"\n#include <stdio.h>\n#include <stddef.h>\n'
                    'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(csm_cfg), sizeof(csm_update),'
-                   ' sizeof(csm_result), sizeof(csm_stats), offsetof(csm_cfg, vertex_headroom));return 0;}')
+                   ' sizeof(csm_result), sizeof(csm_stats), offsetof(csm_cfg, vertex_headroom));'
+                   'printf("%zu\\n", sizeof(csm_index_info));return 0;}')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
-    cfg, upd, res, stats, off = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
+    cfg, upd, res, stats, off, info = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
     assert cfg == ctypes.sizeof(_abi.CsmCfg)
     assert off == _abi.CsmCfg.vertex_headroom.offset
     assert upd == _abi.UPDATE_DTYPE.itemsize == 16
     assert res == _abi.RESULT_DTYPE.itemsize == 48
     assert stats == ctypes.sizeof(_abi.CsmStats)
+    assert info == ctypes.sizeof(_abi.CsmIndexInfo)
 
 
 def test_error_strings_without_a_device():
