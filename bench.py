@@ -35,6 +35,10 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact counts"
+# DRAM bytes (read + write) of one k_search launch over a 4,096-update C3
+# batch, from the ncu capture summarised in profiles/k_search_c3_b4096.md;
+# scaled to a launch by the updates it processes.
+SEARCH_DRAM_BYTES_PER_4096 = 98.4e6
 
 CONFIGS = {
     "c3": {
@@ -384,7 +388,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": B * 16,
                     "d2h_bytes_per_step": B * RESULT_DTYPE.itemsize},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "frac": achieved / peak if peak else None,
+                         "traffic": SEARCH_DRAM_BYTES_PER_4096 * B / 4096 if cfg["preset"] == "c3" else None,
+                         "traffic_note": "ncu dram__bytes_read+write of a 4096-update C3 launch, scaled by updates",
                          "peak_kind": peak_kind, "kernel": "k_search", "launches": search_n,
                          "kernel_ms": search_ms, "algorithmic_bytes": work},
             "cpu_baseline": cpu,
