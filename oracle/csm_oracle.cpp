@@ -85,7 +85,7 @@ struct Graph {
     return elab[x][(size_t)(it - nbr[x].begin())];
   }
   uint32_t seg_size(uint32_t v, uint32_t a, uint32_t l) const {
-    if (a >= n_vl || l >= n_el) return 0;
+    if (!track_seg || a >= n_vl || l >= n_el) return 0;
     return seg[(size_t)v * n_vl * n_el + combo(a, l)];
   }
 };
@@ -611,4 +611,42 @@ extern "C" int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n
     }
   }
   return (int)n;
+}
+
+// InitialMatching (ParaCOSM/CSM/matching/GraphFlow/graphflow.cpp:268-284):
+// every vertex with the label of the first vertex of order 0 starts a
+// FindMatches from depth 1; no per-update cap.  Counted on the graph after
+// the first n_up updates.
+extern "C" int oracle_initial_count(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                                    uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                                    uint64_t n_up, const oracle_update* ups, int homo, uint64_t* count) {
+  QueryGraph q;
+  if (n_qv < 2 || !q.build(n_qv, q_vlabels, n_qe, q_edges) || q.n_edges == 0) return -1;
+  Graph g;
+  for (uint32_t v = 0; v < n_v; v++) g.add_vertex(v, vlabels[v]);
+  if (g.vlabel.size() < n_v) { g.vlabel.resize(n_v, NOT_EXIST); g.nbr.resize(n_v); g.elab.resize(n_v); }
+  for (uint64_t i = 0; i < n_e; i++) {
+    uint32_t a = edges[3 * i], b = edges[3 * i + 1];
+    if (a < n_v && b < n_v && a != b) g.add_edge(a, b, edges[3 * i + 2]);
+  }
+  for (uint64_t i = 0; i < n_up; i++) {
+    const oracle_update& u = ups[i];
+    if (u.type == 'v') { if (u.is_add) g.add_vertex(u.id1, u.label); continue; }
+    if (u.id1 >= g.vlabel.size() || u.id2 >= g.vlabel.size() || u.id1 == u.id2) continue;
+    if (u.is_add) g.add_edge(u.id1, u.id2, u.label); else g.remove_edge(u.id1, u.id2);
+  }
+  std::vector<std::vector<uint32_t>> order;
+  graphflow_orders(q, order);
+  Searcher s(q, g, order, homo != 0, false, 0);
+  s.m.assign(n_qv, NOT_EXIST);
+  s.visited.assign(g.vlabel.size(), 0);
+  const uint32_t u0 = order[0][0];
+  for (uint32_t v = 0; v < g.vlabel.size(); v++) {
+    if (g.vlabel[v] == NOT_EXIST || g.vlabel[v] != q.vlabel[u0]) continue;
+    s.m[u0] = v; s.visited[v] = 1;
+    s.find(0, 1, 0);
+    s.visited[v] = 0; s.m[u0] = NOT_EXIST;
+  }
+  *count = s.count;
+  return 0;
 }

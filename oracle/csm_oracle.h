@@ -78,6 +78,12 @@ int oracle_graphflow_orders(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n
  * parents), d1 / d2 as [n_qv][words] bitsets over data vertex ids.  Returns
  * the number of data vertex ids, or a negative value on bad input. */
 enum { ORACLE_INDEX_TURBOFLUX = 1, ORACLE_INDEX_SYMBI = 2 };
+
+/* Number of embeddings of the query in the graph after the first n_up
+ * updates (InitialMatching, ParaCOSM/CSM/matching/GraphFlow/graphflow.cpp:268-284). */
+int oracle_initial_count(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                         uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                         uint64_t n_up, const oracle_update* ups, int homo, uint64_t* count);
 int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
                  uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
                  uint64_t n_up, const oracle_update* ups, int algo, uint32_t* root, uint32_t* order,

@@ -43,6 +43,10 @@ def lib() -> C.CDLL:
                                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         _lib.oracle_graphflow_orders.restype = C.c_int
         _lib.oracle_graphflow_orders.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        _lib.oracle_initial_count.restype = C.c_int
+        _lib.oracle_initial_count.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                              C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
+                                              C.POINTER(C.c_uint64)]
         _lib.oracle_index.restype = C.c_int
         _lib.oracle_index.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                       C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
@@ -92,6 +96,21 @@ def graphflow_orders(q_vlabels, q_edges) -> np.ndarray:
     if m < 0:
         raise RuntimeError("bad query")
     return out[:m]
+
+
+def initial_count(q_vlabels, q_edges, vlabels, edges, updates=None, *, homo: bool = False) -> int:
+    """Embeddings of the query in the graph after the given updates (InitialMatching)."""
+    qv = np.ascontiguousarray(q_vlabels, dtype=np.uint32)
+    qe = np.ascontiguousarray(q_edges, dtype=np.uint32).reshape(-1, 3)
+    vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+    e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
+    u = np.ascontiguousarray(updates if updates is not None else np.zeros(0, UPDATE_DTYPE), dtype=UPDATE_DTYPE)
+    c = C.c_uint64()
+    rc = lib().oracle_initial_count(len(qv), _p(qv), len(qe), _p(qe), len(vl), _p(vl), len(e), _p(e), len(u), _p(u),
+                                    int(homo), C.byref(c))
+    if rc != 0:
+        raise RuntimeError("oracle_initial_count failed")
+    return int(c.value)
 
 
 INDEX_ALGOS = {"turboflux": 1, "symbi": 2, "parallel_turboflux": 1, "parallel_symbi": 2}

@@ -542,6 +542,126 @@ static int fetch_last(csm_ctx* ctx) {
 
 // ================================================================== C ABI
 
+// ------------------------------------------------------------ initial match
+
+// InitialMatching() (ParaCOSM/CSM/matching/GraphFlow/graphflow.cpp:268-284,
+// SymBi/symbi.cpp:374-402): the number of embeddings of the query in the
+// current graph, without the per-update cap.  Every embedding maps the first
+// anchor query edge (u_a, u_b) onto exactly one directed data entry
+// (m[u_a], m[u_b]), so the entries of S(x, L(u_b), l(u_a, u_b)) over the
+// vertices x of label L(u_a) are the seeds: each becomes a root task of the
+// ordinary search (positions 0 and 1 fixed) and the per-seed counts are summed.
+
+__global__ void k_init_count(DevGraph g, uint32_t la, uint32_t combo, unsigned long long* cnt) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= g.n_cap) return;
+  unsigned long long c = 0;
+  if (v < g.n && g.vlabel[v] == la) {
+    const uint32_t* d = g.dir + (size_t)v * (g.nc + 1) + combo;
+    c = d[1] - d[0];
+  }
+  cnt[v] = c;
+}
+
+// Seeds [first, first + B) of the entry enumeration: info and one task each.
+__global__ void k_init_fill(DevGraph g, uint32_t combo, uint32_t label, const unsigned long long* off,
+                            unsigned long long first, uint32_t B, UpdInfo* info, Task* tasks) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B) return;
+  const unsigned long long e = first + i;
+  uint32_t lo = 0, hi = g.n_cap;  // last x with off[x] <= e
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= e) lo = mid; else hi = mid;
+  }
+  const uint32_t x = lo;
+  const uint32_t* pool = g.pools[g.ps->active];
+  const uint32_t* d = g.dir + (size_t)x * (g.nc + 1) + combo;
+  const uint32_t y = pool[g.row_off[x] + d[0] + (e - off[x])];
+  UpdInfo u;
+  u.v1 = x; u.v2 = y; u.label = label; u.flags = UF_VALID | UF_ADD;
+  info[i] = u;
+  tasks[i] = Task{i, 0, 0, 0};
+}
+
+__global__ void k_init_sum(uint32_t B, const unsigned long long* count, unsigned long long* total) {
+  unsigned long long s = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B; i += gridDim.x * blockDim.x) s += count[i];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(total, s);
+}
+
+static int initial_match(csm_ctx* ctx, uint64_t* out) {
+  cudaStream_t st = ctx->st;
+  DevGraph& g = ctx->g;
+  const PlanAnchor& A = ctx->h_plan->anchors[0];
+  const uint32_t combo = A.lb * g.n_el + A.el;
+  const uint64_t n_cap = g.n_cap;
+  unsigned long long *cnt = nullptr, *off = nullptr, *total = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int64_t)n_cap, st));
+  int rc = ctx->mem.alloc((void**)&cnt, 8ull * n_cap);
+  if (!rc) rc = ctx->mem.alloc((void**)&off, 8ull * n_cap);
+  if (!rc) rc = ctx->mem.alloc((void**)&total, 64);
+  if (!rc) rc = ctx->mem.alloc(&tmp, tb);
+  auto release = [&]() {
+    ctx->mem.release(cnt, 8ull * n_cap); ctx->mem.release(off, 8ull * n_cap);
+    ctx->mem.release(total, 64); ctx->mem.release(tmp, tb);
+  };
+  if (rc) { release(); return rc; }
+  k_init_count<<<blocks_for(n_cap, 256), 256, 0, st>>>(g, A.la, combo, cnt); CKL();
+  CK(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, (int64_t)n_cap, st));
+  CK(cudaMemsetAsync(total, 0, 64, st));
+  unsigned long long last_off = 0, last_cnt = 0;
+  CK(cudaMemcpyAsync(&last_off, off + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&last_cnt, cnt + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const unsigned long long n_seeds = last_off + last_cnt;
+  uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
+  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
+  uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
+  if (!bps) {
+    const size_t smem = search_smem_bytes(ctx->nq, warps);
+    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
+  }
+  for (unsigned long long first = 0; first < n_seeds; first += ctx->bmax) {
+    const uint32_t B = (uint32_t)std::min<unsigned long long>(ctx->bmax, n_seeds - first);
+    unsigned int* c = ctx->d_cnt;
+    CK(cudaMemsetAsync(c, 0, 64, st));
+    CK(cudaMemcpyAsync(c + 6, &B, 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->d_count, 0, 8ull * B, st));
+    CK(cudaMemsetAsync(ctx->d_bytes, 0, 8ull * B, st));
+    CK(cudaMemsetAsync(ctx->d_stop, 0, 4ull * B, st));
+    k_init_fill<<<blocks_for(B, 256), 256, 0, st>>>(g, combo, A.el, off, first, B, ctx->d_info, ctx->d_tasks); CKL();
+    SearchParams sp{};
+    sp.g = g; sp.plan = ctx->d_plan; sp.tasks = ctx->d_tasks; sp.n_tasks = c + 6; sp.task_cap = ctx->task_cap;
+    sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash;
+    sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
+    sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = 0;
+    sp.homo = ctx->cfg.homomorphism; sp.want_hash = 0; sp.error = &g.ps->error;
+    sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.qseq = ctx->d_qseq; sp.qcap = ctx->qcap;
+    sp.wait_limit_ns = 30ull * 1000000000ull;
+    sp.slot_limit_ns = 100ull * 1000000ull;
+    sp.task_limit_ns = 20ull * 1000000000ull;
+    sp.batch = B;
+    sp.sstat = ctx->d_sstat;
+    launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
+    ctx->search_launches++;
+    k_init_sum<<<std::min<uint32_t>(blocks_for(B, 256), 1024), 256, 0, st>>>(B, ctx->d_count, total); CKL();
+    ctx->launches += 3;
+  }
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, total, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  release();
+  rc = check_device_error(ctx);
+  if (rc) return rc;
+  *out = h;
+  return CSM_OK;
+}
+
 extern "C" {
 
 void csm_gpu_default_cfg(csm_cfg* cfg) {
@@ -775,7 +895,11 @@ int csm_gpu_build_index(csm_ctx* ctx) {
 
 int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
   if (!ctx || !count) return set_err(CSM_EINVAL, "null argument");
-  return set_err(CSM_EUNSUPPORTED, "initial matching is not implemented yet");
+  if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
+  CK(cudaSetDevice(ctx->dev));
+  int rc = ensure_batch_buffers(ctx);
+  if (rc) return rc;
+  return initial_match(ctx, count);
 }
 
 int csm_gpu_classify(csm_ctx* ctx, uint64_t n, const csm_update* ups, uint8_t* safe_out) {

@@ -1,0 +1,138 @@
+// Plugin classes over the C ABI (see plugins.h).
+#include "plugins.h"
+
+#include <cstdio>
+
+namespace csm {
+
+matching::matching(const EdgeList& query, const EdgeList& data, size_t max_num_results, bool print_prep,
+                   bool print_enum, bool homo, int algorithm, const GpuOptions& opt)
+    : query_(query), data_(data), max_num_results_(max_num_results), print_preprocessing_results_(print_prep),
+      print_enumeration_results_(print_enum), homomorphism_(homo), algo_(algorithm), opt_(opt) {
+  csm_cfg cfg;
+  csm_gpu_default_cfg(&cfg);
+  cfg.algorithm = algorithm;
+  cfg.homomorphism = homo ? 1 : 0;
+  // the reference's "no cap" is UINT_MAX (main.cpp:681); the engine's is 0
+  cfg.max_results = (max_num_results >= 0xffffffffull) ? 0 : (uint64_t)max_num_results;
+  cfg.mode = opt.mode;
+  cfg.max_batch = opt.max_batch;
+  cfg.want_hash = opt.want_hash ? 1 : 0;
+  cfg.device = opt.device;
+  cfg.turboflux_compat = opt.turboflux_compat ? 1 : 0;
+  cfg.warps_per_block = opt.warps_per_block;
+  cfg.blocks_per_sm = opt.blocks_per_sm;
+  cfg.vertex_headroom = opt.vertex_headroom;
+  cfg.hbm_budget_bytes = opt.hbm_budget_bytes;
+  cfg.deadline_ns = opt.deadline_ns;
+  check(csm_gpu_create(&cfg, &ctx_));
+}
+
+matching::~matching() {
+  if (ctx_) csm_gpu_destroy(ctx_);
+}
+
+int matching::check(int rc) {
+  if (rc != CSM_OK && err_ == CSM_OK) {
+    err_ = rc;
+    const char* t = csm_gpu_last_error();
+    err_text_ = t ? t : csm_gpu_strerror(rc);
+  }
+  return rc;
+}
+
+// BuildDAG + BuildDCS of the reference become: the query and the data graph
+// are copied to the device, then the engine builds its plans and index.
+void matching::Preprocessing() {
+  if (err_) return;
+  if (check(csm_gpu_set_query(ctx_, query_.n, query_.vlabels.data(), (uint32_t)query_.num_edges(),
+                              query_.edges.data())))
+    return;
+  if (check(csm_gpu_load_graph(ctx_, data_.n, data_.vlabels.data(), data_.num_edges(), data_.edges.data()))) return;
+  check(csm_gpu_build_index(ctx_));
+  if (print_preprocessing_results_ && !err_ && algo_ != CSM_ALGO_GRAPHFLOW) {
+    csm_index_info info;
+    if (!check(csm_gpu_index_info(ctx_, &info))) {
+      // the reference's "DAG:" listing (SymBi/symbi.cpp:240-256)
+      printf("DAG: \n");
+      for (uint32_t i = 0; i < info.n_qv; i++) {
+        const uint32_t u = info.order[i];
+        printf("%u: (backwards: ", u);
+        for (uint32_t p = 0; p < info.n_qv; p++)
+          if ((info.parents[u] >> p) & 1u) printf("%u ", p);
+        printf(") (forwards: ");
+        for (uint32_t c = 0; c < info.n_qv; c++)
+          if ((info.parents[c] >> u) & 1u) printf("%u ", c);
+        printf(")\n");
+      }
+      printf("\n");
+    }
+  }
+}
+
+void matching::InitialMatching() {
+  if (err_) return;
+  uint64_t c = 0;
+  if (!check(csm_gpu_initial_match(ctx_, &c))) num_initial_results_ += c;
+}
+
+void matching::run_one(const Update& u) {
+  if (err_) return;
+  csm_update cu;
+  cu.type = u.type; cu.is_add = u.is_add; cu.pad = 0; cu.id1 = u.id1; cu.id2 = u.id2; cu.label = u.label;
+  if (check(csm_gpu_submit(ctx_, 1, &cu))) return;
+  const uint64_t first = seq_++;
+  csm_result r;
+  if (check(csm_gpu_results(ctx_, first, 1, &r))) return;
+  num_positive_results_ += r.pos;
+  num_negative_results_ += r.neg;
+}
+
+void matching::AddEdge(uint32_t v1, uint32_t v2, uint32_t label) { run_one(Update{'e', 1, 0, v1, v2, label}); }
+void matching::RemoveEdge(uint32_t v1, uint32_t v2) { run_one(Update{'e', 0, 0, v1, v2, 0}); }
+void matching::AddVertex(uint32_t id, uint32_t label) { run_one(Update{'v', 1, 0, id, 0, label}); }
+void matching::RemoveVertex(uint32_t id) { run_one(Update{'v', 0, 0, id, 0, 0}); }
+
+bool matching::Classify(uint32_t v1, uint32_t v2, uint32_t label) {
+  csm_update cu{'e', 1, 0, v1, v2, label};
+  uint8_t safe = 0;
+  if (check(csm_gpu_classify(ctx_, 1, &cu, &safe))) return false;
+  return safe != 0;
+}
+
+void matching::GetMemoryCost(size_t& num_edges, size_t& num_vertices) {
+  csm_stats st;
+  num_edges = num_vertices = 0;
+  if (check(csm_gpu_stats(ctx_, &st))) return;
+  num_edges = st.index_entries;
+  num_vertices = st.index_vertices;
+}
+
+int matching::ProcessUpdates(const std::vector<Update>& ups, std::vector<csm_result>& out) {
+  out.resize(ups.size());
+  if (err_) return err_;
+  if (ups.empty()) return CSM_OK;
+  static_assert(sizeof(Update) == sizeof(csm_update), "update records share one layout");
+  if (check(csm_gpu_submit(ctx_, ups.size(), reinterpret_cast<const csm_update*>(ups.data())))) return err_;
+  const uint64_t first = seq_;
+  seq_ += ups.size();
+  if (check(csm_gpu_results(ctx_, first, ups.size(), out.data()))) return err_;
+  for (const csm_result& r : out) {
+    num_positive_results_ += r.pos;
+    num_negative_results_ += r.neg;
+  }
+  return CSM_OK;
+}
+
+matching* make_plugin(const std::string& name, const EdgeList& q, const EdgeList& d, size_t max_results,
+                      bool print_prep, bool print_enum, bool homo, const GpuOptions& opt) {
+  if (name == "parallel_graphflow" || name == "graphflow")
+    return new Parallel_Graphflow(q, d, max_results, print_prep, print_enum, homo, opt);
+  if (name == "parallel_turboflux" || name == "turboflux")
+    return new Parallel_TurboFlux(q, d, max_results, print_prep, print_enum, homo, opt);
+  if (name == "parallel_symbi" || name == "symbi")
+    return new Parrllel_SymBi(q, d, max_results, print_prep, print_enum, homo, opt);
+  return nullptr;
+}
+
+}  // namespace csm

@@ -10,10 +10,13 @@ of sequential SymBi (parsed from its --print-enum output).  index_symbi.txt
 and index_turboflux.txt hold those plugins' own candidate index (root,
 serialized DAG, parents, d1 / d2 flags as little-endian hex bitsets) after
 preprocessing, after half of the stream and after all of it, read out of the
-plugin objects by ref_driver --dump-index.
+plugin objects by ref_driver --dump-index.  initial.json holds the
+InitialMatching count the reference's own csm driver prints for the graph
+before the stream.
 
     python tests/golden/make_golden.py          # needs the reference sources to build the driver
     python tests/golden/make_golden.py --index  # only the index fixtures
+    python tests/golden/make_golden.py --initial  # only initial.json (InitialMatching counts of csm)
 
 Only this script reads the reference; the fixtures it writes are plain files.
 """
@@ -78,7 +81,28 @@ def write_index(d: Path) -> None:
                         f.write(f"{k} {q} {np.packbits(r[k][q], bitorder='little').tobytes().hex()}\n")
 
 
+REF_CSM = ROOT / "oracle" / "_ref" / "csm"
+
+
+def write_initial(d: Path, homo: bool) -> None:
+    """initial.json: the InitialMatching count the reference's own csm driver reports per plugin."""
+    out = {}
+    for algo in ("graphflow", "turboflux", "symbi"):
+        cmd = [str(REF_CSM), "-q", "query.graph", "-d", "data.graph", "-u", "stream.txt", "-a", algo,
+               "--print-prep", "0", "--homo", "1" if homo else "0"]
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=600)
+        lines = r.stdout.splitlines()
+        k = lines.index("----------- Initial Matching ----------")
+        out[algo] = int(lines[k + 2].split()[0])
+    (d / "initial.json").write_text(json.dumps(out) + "\n")
+
+
 def main() -> None:
+    if "--initial" in sys.argv:
+        for name, (_, _, homo) in CASES.items():
+            write_initial(HERE / name, homo)
+            print(name, (HERE / name / "initial.json").read_text().strip())
+        return
     if "--index" in sys.argv:
         for name in CASES:
             write_index(HERE / name)
@@ -129,6 +153,7 @@ def main() -> None:
         (d / "params.json").write_text(json.dumps({"max_results": cap, "homo": homo, "generator": args,
                                                    "plugins": [a for a, _ in PLUGINS if a in cols]}, indent=1))
         write_index(d)
+        write_initial(d, homo)
         print(name, "updates", n, "plugins", list(cols))
 
 

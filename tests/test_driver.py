@@ -1,0 +1,32 @@
+"""The csm driver (paracosm_b200/_bin/csm): the reference's command line and
+output lines over the engine.  CPU checks here; the GPU run is in
+test_gpu_driver.py."""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+CSM = ROOT / "paracosm_b200" / "_bin" / "csm"
+GOLD = Path(__file__).resolve().parent / "golden" / "c1_small"
+
+
+def test_help_lists_the_reference_options():
+    r = subprocess.run([str(CSM), "-h"], capture_output=True, text=True)
+    assert r.returncode == 0
+    for opt in ("-q", "-d", "-u", "-a", "--max-results", "--time-limit", "--print-prep", "--print-enum", "--homo",
+                "--report-initial", "--initial-time-limit", "--orders", "--auto-tuning"):
+        assert opt in r.stderr
+
+
+def test_missing_required_options_fail_without_touching_the_gpu():
+    r = subprocess.run([str(CSM), "-q", "x"], capture_output=True, text=True)
+    assert r.returncode == 2 and "required" in r.stderr
+
+
+def test_unknown_algorithm_is_reported_like_the_reference():
+    r = subprocess.run([str(CSM), "-q", "query.graph", "-d", "data.graph", "-u", "stream.txt", "-a", "nope"],
+                       cwd=GOLD, capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "----------- Loading graphs ------------" in r.stdout and "Unknown algorithm" in r.stdout
+    assert "# vertices = 2048" in r.stdout

@@ -162,3 +162,13 @@ def test_oracle_index_is_the_fixpoint_by_definition():
                 d2[u, v] = d1[u, v] and all(sup(v, qv[c], ql[(u, c)], d2[c]) for c in chd[u])
         assert np.array_equal(o["d1"], d1) and np.array_equal(o["d2"], d2)
         assert o["order"][0] == o["root"] and par[o["root"]] == []
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_oracle_initial_count_matches_the_reference_csm(case):
+    """InitialMatching counts printed by the reference's own csm driver (initial.json)."""
+    import json
+    g = load_golden(case)
+    want = json.loads((g["dir"] / "initial.json").read_text())
+    got = pyoracle.initial_count(g["qv"], g["qe"], g["vl"], g["e"], homo=g["params"]["homo"])
+    assert got == want["graphflow"] == want["symbi"] == want["turboflux"]
