@@ -142,6 +142,29 @@ int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, ui
 int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint64_t n_e,
                        const uint32_t* edges);
 
+/* Standing queries sharing one data graph.  The context that loads the graph
+ * (the owner) folds labels its query does not use into one inert label; to
+ * attach other queries later, first keep their labels distinct with
+ * csm_gpu_reserve_labels (between csm_gpu_set_query and csm_gpu_load_graph).
+ * The reference runs one query per process (main.cpp:676-871); these two
+ * entry points have no reference counterpart. */
+int csm_gpu_reserve_labels(csm_ctx* ctx, uint32_t n_vl, const uint32_t* vlabels, uint32_t n_el,
+                           const uint32_t* elabels);
+
+/* Attaches a standing query to the owner's graph (after the owner's
+ * csm_gpu_build_index), with its own plugin (cfg->algorithm), cap
+ * (cfg->max_results), hash and launch-shape settings; device, mode, batch
+ * size and homomorphism are the owner's.  The new context has its own plan,
+ * candidate index, search buffers and stream.  Updates are submitted to the
+ * owner only: every owner submit applies each mutation once and runs every
+ * attached query on the same batches, their searches overlapping on the
+ * device; each attached context then answers csm_gpu_wait / results / stats /
+ * index calls for its query, with the owner's sequence numbers.  Destroying
+ * an attached context detaches it; destroying the owner leaves attached
+ * contexts without a graph (their calls fail until they are destroyed). */
+int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, const uint32_t* q_vlabels,
+                         uint32_t n_qe, const uint32_t* q_edges, csm_ctx** out);
+
 /* Preprocessing(): matching orders and, for TurboFlux / SymBi, the auxiliary
  * index (BuildDAG + BuildDCS). */
 int csm_gpu_build_index(csm_ctx* ctx);

@@ -96,6 +96,9 @@ _SIGNATURES = [
     ("csm_gpu_create", C.c_int, [C.POINTER(CsmCfg), C.POINTER(C.c_void_p)]),
     ("csm_gpu_set_query", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("csm_gpu_load_graph", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("csm_gpu_reserve_labels", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("csm_gpu_attach_query", C.c_int, [C.c_void_p, C.POINTER(CsmCfg), C.c_uint32, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.POINTER(C.c_void_p)]),
     ("csm_gpu_build_index", C.c_int, [C.c_void_p]),
     ("csm_gpu_initial_match", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("csm_gpu_classify", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),

@@ -117,6 +117,11 @@ struct csm_ctx {
   size_t sev_used = 0;
   uint64_t search_launches = 0, work_bytes = 0;
   double search_ms = 0;
+  // standing queries sharing one data graph: the owner holds the graph and
+  // applies mutations; attached contexts hold a query, its plan and index
+  csm_ctx* owner = nullptr;
+  std::vector<csm_ctx*> attached;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace csm {
@@ -310,22 +315,26 @@ __global__ void k_latency(uint32_t B, const unsigned long long* stamp, csm_resul
   out[s].latency_ns = t - stamp[0];
 }
 
-// Launch sequence of one batch of B edge updates already in device memory.
-static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_result* out) {
+// ------------------------------------------------------------ batches
+//
+// One batch of B edge updates runs in phases.  The context that owns the
+// data graph applies the insertions (the union graph), every standing query
+// -- the owner's and those attached to it, each on its own stream -- brings
+// its index to the union graph and searches, then the owner applies the
+// deletions and every query brings its index to the graph after the batch.
+// Events order the streams; the searches of different queries overlap.
+
+// Owner: group the batch's updates per edge, resolve each edge's timeline,
+// temporal entries, CSR -> union graph.
+static int batch_mutate_insert(csm_ctx* ctx, const csm_update* ups, uint32_t B, uint32_t L) {
   cudaStream_t st = ctx->st;
   DevGraph& g = ctx->g;
-  const uint32_t L = std::min<uint32_t>(ctx->lcap, 4 * B + 64);
   const KeyBits kb = g.kb;
   CK(cudaMemsetAsync(ctx->d_cnt, 0, 64, st));
   CK(cudaMemsetAsync(ctx->d_ins, 0xff, 8ull * L, st));
   CK(cudaMemsetAsync(ctx->d_del, 0xff, 8ull * L, st));
   CK(cudaMemsetAsync(ctx->d_tk, 0xff, 8ull * L, st));
-  CK(cudaMemsetAsync(ctx->d_count, 0, 8ull * B, st));
-  CK(cudaMemsetAsync(ctx->d_bytes, 0, 8ull * B, st));
-  CK(cudaMemsetAsync(ctx->d_stop, 0, 4ull * B, st));
-  if (ctx->cfg.want_hash) CK(cudaMemsetAsync(ctx->d_hash, 0, 8ull * B, st));
   unsigned int* c = ctx->d_cnt;
-
   k_batch_init<<<blocks_for(B, 256), 256, 0, st>>>(ups, B, g, ctx->d_ukey, ctx->d_useq, ctx->d_info); CKL();
   size_t tb = ctx->cub_bytes;
   CK(cub::DeviceRadixSort::SortPairs(ctx->d_cub, tb, ctx->d_ukey, ctx->d_ukey2, ctx->d_useq, ctx->d_useq2, (int)B, 0, 64, st));
@@ -351,71 +360,164 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   k_compact_finish<<<1, 1, 0, st>>>(g); CKL();
   const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
   k_mut_insert<<<mut_blocks, 256, 0, st>>>(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g); CKL();
-  // candidate index: union-graph insertions
-  int rc = index_apply_edges(ctx->index, g, ctx->d_ins2, L, st, &ctx->launches);
+  return CSM_OK;
+}
+
+static void search_shape(const csm_ctx* q, uint32_t& warps, uint32_t& bps) {
+  warps = q->cfg.warps_per_block ? q->cfg.warps_per_block : 8;
+  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
+  bps = q->cfg.blocks_per_sm ? q->cfg.blocks_per_sm : 0;
+  if (!bps) {
+    const size_t smem = search_smem_bytes(q->nq, warps);
+    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
+  }
+}
+
+// One standing query q over the owner o's union graph: index to the union
+// graph, seeds, search, per-update results; on q's stream.
+static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, csm_result* out) {
+  csm_ctx* ctx = q;  // launches are counted on the query's context
+  cudaStream_t st = q->st;
+  const DevGraph& g = o->g;
+  CK(cudaMemsetAsync(q->d_count, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(q->d_bytes, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(q->d_stop, 0, 4ull * B, st));
+  if (q->cfg.want_hash) CK(cudaMemsetAsync(q->d_hash, 0, 8ull * B, st));
+  unsigned int* c = q->d_cnt;
+  if (q != o) CK(cudaMemsetAsync(c, 0, 64, st));
+  int rc = index_apply_edges(q->index, g, o->d_ins2, L, st, &q->launches);
   if (rc) return rc;
-  // search
-  k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, ctx->d_info, g, ctx->d_plan, ctx->index.d2, ctx->index.words,
-                                              ctx->d_tasks, c + 6, ctx->task_cap, ctx->d_safe, &g.ps->error); CKL();
+  k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, o->d_info, g, q->d_plan, q->index.d2, q->index.words,
+                                              q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error); CKL();
   SearchParams sp{};
-  sp.g = g; sp.plan = ctx->d_plan; sp.tasks = ctx->d_tasks; sp.n_tasks = c + 6; sp.task_cap = ctx->task_cap;
-  sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash; sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
-  sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = ctx->cfg.max_results;
-  sp.homo = ctx->cfg.homomorphism; sp.want_hash = ctx->cfg.want_hash; sp.error = &g.ps->error;
-  sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.qseq = ctx->d_qseq; sp.qcap = ctx->qcap;
+  sp.g = g; sp.plan = q->d_plan; sp.tasks = q->d_tasks; sp.n_tasks = c + 6; sp.task_cap = q->task_cap;
+  sp.task_next = c + 7; sp.info = o->d_info; sp.count = q->d_count; sp.hash = q->d_hash; sp.bytes = q->d_bytes;
+  sp.stop = q->d_stop;
+  sp.d2 = q->index.d2; sp.d2_words = q->index.words; sp.cap = q->cfg.max_results;
+  sp.homo = q->cfg.homomorphism; sp.want_hash = q->cfg.want_hash; sp.error = &g.ps->error;
+  sp.q = q->d_q; sp.dq = q->d_dq; sp.qseq = q->d_qseq; sp.qcap = q->qcap;
   sp.wait_limit_ns = 30ull * 1000000000ull;
   sp.slot_limit_ns = 100ull * 1000000ull;
   sp.task_limit_ns = 20ull * 1000000000ull;
   sp.batch = B;
-  sp.sstat = ctx->d_sstat;
-  uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
-  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
-  uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
-  if (!bps) {
-    const size_t smem = search_smem_bytes(ctx->nq, warps);
-    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
-  }
-  if (ctx->sev_used == ctx->sev.size()) {
+  sp.sstat = q->d_sstat;
+  uint32_t warps, bps;
+  search_shape(q, warps, bps);
+  if (q->sev_used == q->sev.size()) {
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
-    ctx->sev.emplace_back(a, b);
+    q->sev.emplace_back(a, b);
   }
-  CK(cudaEventRecord(ctx->sev[ctx->sev_used].first, st));
-  launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
-  CK(cudaEventRecord(ctx->sev[ctx->sev_used].second, st));
-  ctx->sev_used++;
-  k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, ctx->d_info, ctx->d_count, ctx->d_hash, ctx->d_bytes,
-                                                  ctx->d_safe, ctx->cfg.max_results, ctx->cfg.want_hash, out); CKL();
-  k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, ctx->d_stamp, out); CKL();
-  // union graph -> CSR after the batch
+  CK(cudaEventRecord(q->sev[q->sev_used].first, st));
+  launch_search(sp, q->nq, (uint32_t)q->sm_count * bps, warps, st); CKL();
+  CK(cudaEventRecord(q->sev[q->sev_used].second, st));
+  q->sev_used++;
+  k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_info, q->d_count, q->d_hash, q->d_bytes,
+                                                  q->d_safe, q->cfg.max_results, q->cfg.want_hash, out); CKL();
+  k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_stamp, out); CKL();
+  return CSM_OK;
+}
+
+// Stream `waiter` continues after the work queued so far on `signaller`.
+static int stream_after(cudaStream_t waiter, cudaStream_t signaller, cudaEvent_t ev) {
+  CK(cudaEventRecord(ev, signaller));
+  CK(cudaStreamWaitEvent(waiter, ev, 0));
+  return CSM_OK;
+}
+
+// Launch sequence of one batch of B edge updates already in device memory;
+// out_q[k] is the result array of attached query k (in ctx->attached order).
+static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_result* out,
+                          const std::vector<csm_result*>& out_q) {
+  cudaStream_t st = ctx->st;
+  const uint32_t L = std::min<uint32_t>(ctx->lcap, 4 * B + 64);
+  int rc = batch_mutate_insert(ctx, ups, B, L);
+  if (rc) return rc;
+  // every query: index to the union graph, then search
+  for (size_t k = 0; k < ctx->attached.size(); k++) {
+    csm_ctx* a = ctx->attached[k];
+    a->g = ctx->g;
+    rc = stream_after(a->st, st, ctx->ev_fork);
+    if (!rc) rc = batch_query_search(a, ctx, B, L, out_q[k]);
+    if (rc) return rc;
+  }
+  rc = batch_query_search(ctx, ctx, B, L, out);
+  if (rc) return rc;
+  for (csm_ctx* a : ctx->attached) {
+    rc = stream_after(st, a->st, a->ev_join);
+    if (rc) return rc;
+  }
+  // union graph -> CSR after the batch, and every index to it
+  unsigned int* c = ctx->d_cnt;
+  DevGraph& g = ctx->g;
+  const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
   k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, g); CKL();
+  for (csm_ctx* a : ctx->attached) {
+    rc = stream_after(a->st, st, ctx->ev_fork);
+    if (!rc) rc = index_apply_edges(a->index, g, ctx->d_del2, L, a->st, &a->launches);
+    if (rc) return rc;
+  }
+  for (csm_ctx* a : ctx->attached) {
+    rc = stream_after(st, a->st, a->ev_join);
+    if (rc) return rc;
+  }
   rc = index_apply_edges(ctx->index, g, ctx->d_del2, L, st, &ctx->launches);
   if (rc) return rc;
   k_temporal_clear<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
   ctx->batches++;
+  for (csm_ctx* a : ctx->attached) a->batches++;
   return CSM_OK;
 }
 
-static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_update& h, csm_result* out) {
+static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_update& h, csm_result* out,
+                             const std::vector<csm_result*>& out_q) {
   cudaStream_t st = ctx->st;
   if (h.is_add && h.id1 < ctx->g.n_cap && h.id1 >= ctx->g.n) ctx->g.n = h.id1 + 1;
   k_vertex_update<<<1, 32, 0, st>>>(ups, 1, ctx->g, ctx->d_info); CKL();
   CK(cudaMemsetAsync(ctx->d_safe, 0xff, 4, st));
   k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, 0, 0, out); CKL();
   int rc = index_vertex_update(ctx->index, ctx->g, h, st, &ctx->launches);
-  return rc;
+  if (rc) return rc;
+  for (size_t k = 0; k < ctx->attached.size(); k++) {
+    csm_ctx* a = ctx->attached[k];
+    a->g = ctx->g;
+    rc = stream_after(a->st, st, ctx->ev_fork);
+    if (rc) return rc;
+    k_finalize<<<1, 32, 0, a->st>>>(1, ctx->d_info, a->d_count, a->d_hash, nullptr, nullptr, 0, 0, out_q[k]);
+    a->launches++;
+    CK(cudaGetLastError());
+    rc = index_vertex_update(a->index, ctx->g, h, a->st, &a->launches);
+    if (rc) return rc;
+  }
+  for (csm_ctx* a : ctx->attached) {
+    rc = stream_after(st, a->st, a->ev_join);
+    if (rc) return rc;
+  }
+  return CSM_OK;
 }
 
 static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, const csm_update* h_ups) {
+  if (ctx->owner) return set_err(CSM_ESTATE, "updates of an attached query are submitted to its owner");
   if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
   int rc = ensure_batch_buffers(ctx);
   if (rc) return rc;
   rc = ensure_results(ctx, n);
   if (rc) return rc;
   cudaStream_t st = ctx->st;
+  for (csm_ctx* a : ctx->attached) {
+    rc = ensure_results(a, n);
+    if (!rc) rc = stream_after(st, a->st, a->ev_join);  // work issued on it outside a submit
+    if (rc) return rc;
+  }
   CK(cudaEventRecord(ctx->ev_start, st));
   k_stamp<<<1, 1, 0, st>>>(ctx->d_stamp); CKL();
+  for (csm_ctx* a : ctx->attached) {
+    rc = stream_after(a->st, st, ctx->ev_fork);
+    if (rc) return rc;
+    CK(cudaEventRecord(a->ev_start, a->st));
+  }
+  std::vector<csm_result*> out_q(ctx->attached.size());
   const uint32_t B = (ctx->cfg.mode == CSM_MODE_PLAIN) ? 1u : ctx->bmax;
   // vertex updates run on their own; runs of edge updates form batches
   std::vector<csm_update> hv;
@@ -428,27 +530,35 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
   }
   uint64_t i = 0;
   while (i < n) {
+    for (size_t k = 0; k < ctx->attached.size(); k++) out_q[k] = ctx->attached[k]->d_results + i;
     if (h[i].type == 'v') {
-      rc = run_vertex_update(ctx, d_ups + i, h[i], ctx->d_results + i);
+      rc = run_vertex_update(ctx, d_ups + i, h[i], ctx->d_results + i, out_q);
       if (rc) return rc;
       ctx->v_updates++;
+      for (csm_ctx* a : ctx->attached) a->v_updates++;
       i++;
       continue;
     }
     uint64_t j = i;
     while (j < n && j - i < B && h[j].type != 'v') j++;
-    rc = run_edge_batch(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i);
+    rc = run_edge_batch(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i, out_q);
     if (rc) return rc;
     ctx->e_updates += j - i;
+    for (csm_ctx* a : ctx->attached) a->e_updates += j - i;
     i = j;
   }
   CK(cudaEventRecord(ctx->ev_end, st));
-  ctx->last_first = ctx->seq_next;
-  ctx->last_n = n;
-  ctx->seq_next += n;
-  ctx->updates_done += n;
-  ctx->totals_dirty = true;
-  ctx->h_last_valid = false;
+  std::vector<csm_ctx*> all{ctx};
+  all.insert(all.end(), ctx->attached.begin(), ctx->attached.end());
+  for (csm_ctx* q : all) {
+    if (q != ctx) CK(cudaEventRecord(q->ev_end, q->st));
+    q->last_first = q->seq_next;
+    q->last_n = n;
+    q->seq_next += n;
+    q->updates_done += n;
+    q->totals_dirty = true;
+    q->h_last_valid = false;
+  }
   return CSM_OK;
 }
 
@@ -708,7 +818,9 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   cudaMemGetInfo(&free_b, &total_b);
   ctx->mem.budget = cfg->hbm_budget_bytes ? cfg->hbm_budget_bytes : (uint64_t)(0.9 * (double)free_b);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_end) != cudaSuccess) {
+      cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_end) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete ctx;
     return set_err(CSM_ECUDA, "stream/event creation failed");
   }
@@ -717,9 +829,9 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   return CSM_OK;
 }
 
-int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges) {
-  if (!ctx || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
-  if (ctx->has_graph) return set_err(CSM_ESTATE, "set the query before loading the graph");
+// Query graph of a context: sorted adjacency like Graph::AddEdge (repeats
+// ignored), connectivity and size limits.  Label folding is set by the caller.
+static int parse_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges) {
   if (n_qv < 2 || n_qv > kMaxQ) return set_err(CSM_EUNSUPPORTED, "query must have 2..%u vertices", kMaxQ);
   ctx->nq = n_qv;
   ctx->qvl.assign(q_vlabels, q_vlabels + n_qv);
@@ -741,16 +853,6 @@ int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, ui
     ctx->qe.push_back(a); ctx->qe.push_back(b); ctx->qe.push_back(l);
   }
   if (ctx->qe.empty()) return set_err(CSM_EINVAL, "query has no edges");
-  ctx->qlab_v = ctx->qvl;
-  std::sort(ctx->qlab_v.begin(), ctx->qlab_v.end());
-  ctx->qlab_v.erase(std::unique(ctx->qlab_v.begin(), ctx->qlab_v.end()), ctx->qlab_v.end());
-  ctx->qlab_e.clear();
-  for (size_t i = 0; i < ctx->qe.size(); i += 3) ctx->qlab_e.push_back(ctx->qe[i + 2]);
-  std::sort(ctx->qlab_e.begin(), ctx->qlab_e.end());
-  ctx->qlab_e.erase(std::unique(ctx->qlab_e.begin(), ctx->qlab_e.end()), ctx->qlab_e.end());
-  if (ctx->qlab_e.size() + 1 > 64) return set_err(CSM_EUNSUPPORTED, "at most 63 distinct query edge labels");
-  ctx->qvl_f.resize(n_qv);
-  for (uint32_t u = 0; u < n_qv; u++) ctx->qvl_f[u] = fold_host(ctx->qlab_v, ctx->qvl[u]);
   {  // the edge-anchored search needs a connected query
     std::vector<char> seen(n_qv, 0);
     std::vector<uint32_t> stack{0};
@@ -763,7 +865,115 @@ int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, ui
     if (reached != n_qv) return set_err(CSM_EUNSUPPORTED, "query graph is not connected");
   }
   if (ctx->qe.size() / 3 > kMaxQE) return set_err(CSM_EUNSUPPORTED, "query has more than %u edges", kMaxQE);
+  return CSM_OK;
+}
+
+// Folded query labels from the context's folding tables.
+static void fold_query(csm_ctx* ctx) {
+  ctx->qvl_f.resize(ctx->nq);
+  for (uint32_t u = 0; u < ctx->nq; u++) ctx->qvl_f[u] = fold_host(ctx->qlab_v, ctx->qvl[u]);
+}
+
+int csm_gpu_set_query(csm_ctx* ctx, uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges) {
+  if (!ctx || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
+  if (ctx->owner) return set_err(CSM_ESTATE, "an attached query is set by csm_gpu_attach_query");
+  if (ctx->has_graph) return set_err(CSM_ESTATE, "set the query before loading the graph");
+  int rc = parse_query(ctx, n_qv, q_vlabels, n_qe, q_edges);
+  if (rc) return rc;
+  ctx->qlab_v = ctx->qvl;
+  std::sort(ctx->qlab_v.begin(), ctx->qlab_v.end());
+  ctx->qlab_v.erase(std::unique(ctx->qlab_v.begin(), ctx->qlab_v.end()), ctx->qlab_v.end());
+  ctx->qlab_e.clear();
+  for (size_t i = 0; i < ctx->qe.size(); i += 3) ctx->qlab_e.push_back(ctx->qe[i + 2]);
+  std::sort(ctx->qlab_e.begin(), ctx->qlab_e.end());
+  ctx->qlab_e.erase(std::unique(ctx->qlab_e.begin(), ctx->qlab_e.end()), ctx->qlab_e.end());
+  if (ctx->qlab_e.size() + 1 > 64) return set_err(CSM_EUNSUPPORTED, "at most 63 distinct query edge labels");
+  fold_query(ctx);
   ctx->has_query = true;
+  return CSM_OK;
+}
+
+int csm_gpu_reserve_labels(csm_ctx* ctx, uint32_t n_vl, const uint32_t* vlabels, uint32_t n_el, const uint32_t* elabels) {
+  if (!ctx || (n_vl && !vlabels) || (n_el && !elabels)) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->has_query || ctx->owner) return set_err(CSM_ESTATE, "set the query of an owning context first");
+  if (ctx->has_graph) return set_err(CSM_ESTATE, "reserve labels before loading the graph");
+  for (uint32_t i = 0; i < n_vl; i++) {
+    if (vlabels[i] == kNone) return set_err(CSM_EINVAL, "label 0xffffffff is reserved for absent vertices");
+    ctx->qlab_v.push_back(vlabels[i]);
+  }
+  for (uint32_t i = 0; i < n_el; i++) ctx->qlab_e.push_back(elabels[i]);
+  std::sort(ctx->qlab_v.begin(), ctx->qlab_v.end());
+  ctx->qlab_v.erase(std::unique(ctx->qlab_v.begin(), ctx->qlab_v.end()), ctx->qlab_v.end());
+  std::sort(ctx->qlab_e.begin(), ctx->qlab_e.end());
+  ctx->qlab_e.erase(std::unique(ctx->qlab_e.begin(), ctx->qlab_e.end()), ctx->qlab_e.end());
+  if (ctx->qlab_e.size() + 1 > 64) return set_err(CSM_EUNSUPPORTED, "at most 63 distinct edge labels");
+  if (ctx->qlab_v.size() + 1 > 4096) return set_err(CSM_EUNSUPPORTED, "at most 4095 distinct vertex labels");
+  fold_query(ctx);
+  return CSM_OK;
+}
+
+int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, const uint32_t* q_vlabels,
+                         uint32_t n_qe, const uint32_t* q_edges, csm_ctx** out) {
+  if (!owner || !cfg || !out || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
+  if (owner->owner) return set_err(CSM_ESTATE, "attach to the context that owns the graph");
+  if (!owner->has_graph || !owner->has_plan) return set_err(CSM_ESTATE, "the owner needs a graph and a built index");
+  if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
+  CK(cudaSetDevice(owner->dev));
+  CK(cudaStreamSynchronize(owner->st));
+  csm_ctx* a = new csm_ctx();
+  a->cfg = owner->cfg;
+  a->cfg.algorithm = cfg->algorithm;
+  a->cfg.max_results = cfg->max_results;
+  a->cfg.want_hash = cfg->want_hash;
+  a->cfg.warps_per_block = cfg->warps_per_block;
+  a->cfg.blocks_per_sm = cfg->blocks_per_sm;
+  a->cfg.turboflux_compat = cfg->turboflux_compat;
+  a->cfg.hbm_budget_bytes = cfg->hbm_budget_bytes;
+  a->bmax = owner->bmax;
+  a->dev = owner->dev;
+  a->sm_count = owner->sm_count;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  a->mem.budget = cfg->hbm_budget_bytes ? cfg->hbm_budget_bytes : (uint64_t)(0.9 * (double)free_b);
+  auto fail = [&](int rc) { csm_gpu_destroy(a); return rc; };
+  if (cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&a->ev_start) != cudaSuccess || cudaEventCreate(&a->ev_end) != cudaSuccess ||
+      cudaEventCreateWithFlags(&a->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&a->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return fail(set_err(CSM_ECUDA, "stream/event creation failed"));
+  a->h_plan = new Plan();
+  int rc = parse_query(a, n_qv, q_vlabels, n_qe, q_edges);
+  if (rc) return fail(rc);
+  // the owner's label folding: every label of this query must be one it keeps
+  a->qlab_v = owner->qlab_v;
+  a->qlab_e = owner->qlab_e;
+  fold_query(a);
+  for (uint32_t u = 0; u < a->nq; u++)
+    if (a->qvl_f[u] == (uint32_t)a->qlab_v.size())
+      return fail(set_err(CSM_EUNSUPPORTED, "vertex label %u is not kept by the owner (csm_gpu_reserve_labels)",
+                          a->qvl[u]));
+  for (size_t i = 0; i < a->qe.size(); i += 3)
+    if (fold_host(a->qlab_e, a->qe[i + 2]) == (uint32_t)a->qlab_e.size())
+      return fail(set_err(CSM_EUNSUPPORTED, "edge label %u is not kept by the owner (csm_gpu_reserve_labels)",
+                          a->qe[i + 2]));
+  a->has_query = true;
+  a->g = owner->g;
+  a->has_graph = true;
+  a->num_edges = owner->num_edges;
+  rc = build_plan(a);
+  if (!rc) rc = ensure_batch_buffers(a);
+  if (!rc) {
+    std::vector<std::vector<uint32_t>> qel_f(a->nq);
+    for (uint32_t u = 0; u < a->nq; u++)
+      for (uint32_t l : a->qel[u]) qel_f[u].push_back(fold_host(a->qlab_e, l));
+    IndexQuery q{a->nq, &a->qvl_f, &a->qnbr, &qel_f};
+    rc = index_build(a->index, a->mem, a->g, q, a->cfg.algorithm, a->sm_count, a->st, &a->launches);
+  }
+  if (rc) return fail(rc);
+  a->seq_next = owner->seq_next;
+  a->owner = owner;
+  owner->attached.push_back(a);
+  *out = a;
   return CSM_OK;
 }
 
@@ -777,6 +987,7 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
   const uint32_t n_vl = (uint32_t)ctx->qlab_v.size() + 1;
   const uint32_t n_el = (uint32_t)ctx->qlab_e.size() + 1;
   const uint64_t nc = (uint64_t)n_vl * n_el;
+  if (nc > 65535) return set_err(CSM_EUNSUPPORTED, "%llu label combinations (at most 65535)", (unsigned long long)nc);
   const uint32_t headroom = ctx->cfg.vertex_headroom ? ctx->cfg.vertex_headroom : 1024;
   const uint64_t n_cap64 = (uint64_t)n_v + headroom;
   if (n_cap64 > (1ull << 30)) return set_err(CSM_EUNSUPPORTED, "too many vertices");
@@ -899,6 +1110,11 @@ int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
   CK(cudaSetDevice(ctx->dev));
   int rc = ensure_batch_buffers(ctx);
   if (rc) return rc;
+  if (ctx->owner) {  // an attached query reads the owner's graph after the owner's queued work
+    ctx->g = ctx->owner->g;
+    rc = stream_after(ctx->st, ctx->owner->st, ctx->ev_fork);
+    if (rc) return rc;
+  }
   return initial_match(ctx, count);
 }
 
@@ -1069,6 +1285,17 @@ void csm_gpu_destroy(csm_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->dev);
   cudaStreamSynchronize(ctx->st);
+  if (ctx->owner) {  // an attached query leaves its owner's list
+    auto& v = ctx->owner->attached;
+    v.erase(std::remove(v.begin(), v.end(), ctx), v.end());
+  }
+  for (csm_ctx* a : ctx->attached) {  // attached queries lose their graph; their calls then fail
+    cudaStreamSynchronize(a->st);
+    a->owner = nullptr;
+    a->has_graph = false;
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   index_free(ctx->index, ctx->mem);
   ctx->mem.free_all();
   for (auto& e : ctx->sev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }

@@ -60,6 +60,8 @@ class Engine:
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))
         self.h = h
         self.submitted = 0
+        self.attached: list[Engine] = []
+        self.owner: Engine | None = None
 
     # -- setup ---------------------------------------------------------
     def set_query(self, vlabels, edges) -> None:
@@ -72,8 +74,34 @@ class Engine:
         e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
         check(self.lib, self.lib.csm_gpu_load_graph(self.h, len(vl), _ptr(vl), len(e), _ptr(e)))
 
+    def reserve_labels(self, vlabels=(), elabels=()) -> None:
+        """Keeps these labels distinct (for queries attached later); before load_graph."""
+        vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+        el = np.ascontiguousarray(elabels, dtype=np.uint32)
+        check(self.lib, self.lib.csm_gpu_reserve_labels(self.h, len(vl), _ptr(vl), len(el), _ptr(el)))
+
     def build_index(self) -> None:
         check(self.lib, self.lib.csm_gpu_build_index(self.h))
+
+    def attach(self, vlabels, edges, algorithm: str | int = "parallel_graphflow", *, max_results: int = 0,
+               want_hash: bool = False, warps_per_block: int = 0, blocks_per_sm: int = 0) -> "Engine":
+        """A standing query on this engine's graph; its results follow every submit to this engine."""
+        cfg = CsmCfg()
+        self.lib.csm_gpu_default_cfg(C.byref(cfg))
+        cfg.algorithm = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        cfg.max_results = int(max_results)
+        cfg.want_hash = int(bool(want_hash))
+        cfg.warps_per_block = int(warps_per_block)
+        cfg.blocks_per_sm = int(blocks_per_sm)
+        vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+        e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
+        h = C.c_void_p()
+        check(self.lib, self.lib.csm_gpu_attach_query(self.h, C.byref(cfg), len(vl), _ptr(vl), len(e), _ptr(e),
+                                                      C.byref(h)))
+        a = Engine.__new__(Engine)
+        a.lib, a.cfg, a.h, a.submitted, a.attached, a.owner = self.lib, cfg, h, self.submitted, [], self
+        self.attached.append(a)
+        return a
 
     def initial_match(self) -> int:
         c = C.c_uint64()
@@ -93,22 +121,27 @@ class Engine:
             np.ascontiguousarray(updates, dtype=UPDATE_DTYPE)
         first = self.submitted
         check(self.lib, self.lib.csm_gpu_submit(self.h, len(u), _ptr(u)))
-        self.submitted += len(u)
+        self._advance(len(u))
         return first
 
     def submit_ptr(self, ptr: int, n: int) -> int:
         """Queues n updates from a raw host pointer (e.g. pinned memory)."""
         first = self.submitted
         check(self.lib, self.lib.csm_gpu_submit(self.h, n, ptr))
-        self.submitted += n
+        self._advance(n)
         return first
 
     def submit_device(self, dptr: int, n: int) -> int:
         """Queues n updates already in device memory (e.g. a CUDA tensor's data_ptr())."""
         first = self.submitted
         check(self.lib, self.lib.csm_gpu_submit_device(self.h, n, dptr))
-        self.submitted += n
+        self._advance(n)
         return first
+
+    def _advance(self, n: int) -> None:
+        self.submitted += n
+        for a in self.attached:
+            a.submitted += n
 
     def wait(self, timeout_ns: int = 0) -> None:
         check(self.lib, self.lib.csm_gpu_wait(self.h, timeout_ns))
@@ -168,6 +201,8 @@ class Engine:
 
     def close(self) -> None:
         if getattr(self, "h", None):
+            if self.owner is not None and self in self.owner.attached:
+                self.owner.attached.remove(self)
             self.lib.csm_gpu_destroy(self.h)
             self.h = None
 
