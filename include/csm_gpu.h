@@ -172,6 +172,17 @@ int csm_gpu_build_index(csm_ctx* ctx);
 /* InitialMatching(): number of embeddings in the current graph. */
 int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count);
 
+/* Autotuner: times the search on n sample edges (host memory, type 'e'
+ * records; searched as insertions into the current graph, which is not
+ * modified) for every launch shape the SM admits -- warps per block x
+ * resident blocks per SM -- and keeps the fastest for this context's later
+ * searches.  Reports the shape and its search time on the sample.  The
+ * reference tunes its CPU thread count instead (--auto-tuning,
+ * ParaCOSM/CSM/matching/Parallel_TurboFlux/parallel_turboflux.cpp); there is
+ * no counterpart entry point. */
+int csm_gpu_autotune(csm_ctx* ctx, uint32_t n, const csm_update* edges, uint32_t* warps_per_block,
+                     uint32_t* blocks_per_sm, float* search_ms);
+
 /* Classify(v1, v2, label) for n updates: safe_out[i] = 1 when no query edge
  * matches the label triple (L(v1), L(v2), label) in either orientation
  * (ParaCOSM/CSM/matching/Parallel_GraphFlow/parallel_graphflow.cpp:1990-2016). */

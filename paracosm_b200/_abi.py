@@ -101,6 +101,8 @@ _SIGNATURES = [
                                        C.c_void_p, C.POINTER(C.c_void_p)]),
     ("csm_gpu_build_index", C.c_int, [C.c_void_p]),
     ("csm_gpu_initial_match", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("csm_gpu_autotune", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     ("csm_gpu_classify", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("csm_gpu_submit", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
     ("csm_gpu_submit_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),

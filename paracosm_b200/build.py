@@ -5,6 +5,7 @@
 Outputs (git-ignored, but they travel with the working tree):
     paracosm_b200/_lib/libcsmgpu.so   CUDA engine behind include/csm_gpu.h (sm_100a)
     paracosm_b200/_bin/csm            csm driver (reference command line) over the engine
+    paracosm_b200/_bin/csm_serve      serving loop (standing queries, streamed updates, continuous batching)
     paracosm_b200/_bin/csm_gen        seeded workload generator
     oracle/_build/                    CPU restatement used as the checker
     oracle/_ref/                      the reference compiled from its sources (checker / CPU baseline)
@@ -75,6 +76,13 @@ def build_host(force: bool = False) -> None:
     gen_src = [HOST / "csm_gen.cpp", HOST / "workload.cpp"] + common
     if force or _stale(gen, gen_src + [HOST / "workload.h", HOST / "graph_io.h"]):
         _run([CXX, "-std=c++17", "-O3", "-fopenmp", "-o", str(gen)] + [str(s) for s in gen_src])
+    link = ["-L", str(LIB), "-lcsmgpu", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN/../_lib"]
+    srv = BIN / "csm_serve"
+    srv_src = [HOST / "csm_serve.cpp", HOST / "serve.cpp"] + common
+    deps = srv_src + [HOST / "serve.h", HOST / "graph_io.h", ROOT / "include" / "csm_gpu.h", LIB / "libcsmgpu.so"]
+    if force or _stale(srv, deps):
+        _run([CXX, "-std=c++17", "-O3", "-pthread", "-I", str(ROOT / "include"), "-o", str(srv)]
+             + [str(s) for s in srv_src] + link)
     drv = BIN / "csm"
     drv_src = [HOST / "csm_main.cpp", HOST / "plugins.cpp"] + common
     if (HOST / "csm_main.cpp").exists():

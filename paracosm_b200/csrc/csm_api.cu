@@ -652,6 +652,88 @@ static int fetch_last(csm_ctx* ctx) {
 
 // ================================================================== C ABI
 
+// ------------------------------------------------------------ autotuner
+//
+// The search's launch shape -- warps per block (each warp walks one subtree
+// at a time, so this sets how many subtrees share a block's shared memory)
+// and resident blocks per SM -- is chosen per query and graph by timing the
+// search on a sample of update edges for every shape the SM admits (shared
+// memory of the per-warp level buffers, 32 warps of 64 registers per SM).
+// The sample is searched as insertions against the current graph, which is
+// not modified: each edge's seeds run the ordinary search with positions 0
+// and 1 fixed, whether or not the edge is present.
+
+__global__ void k_tune_prep(const csm_update* edges, uint32_t n, DevGraph g, UpdInfo* info) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const csm_update u = edges[i];
+  UpdInfo inf;
+  inf.v1 = u.id1; inf.v2 = u.id2; inf.label = fold_elabel(g, u.label);
+  const bool ok = u.type == 'e' && u.id1 < g.n && u.id2 < g.n && u.id1 != u.id2 && g.vlabel[u.id1] != kNone &&
+                  g.vlabel[u.id2] != kNone;
+  inf.flags = ok ? (UF_VALID | UF_ADD) : UF_INVALID;
+  info[i] = inf;
+}
+
+static int tune_run(csm_ctx* ctx, uint32_t B, uint32_t warps, uint32_t bps, float* ms) {
+  cudaStream_t st = ctx->st;
+  const DevGraph& g = ctx->g;
+  unsigned int* c = ctx->d_cnt;
+  CK(cudaMemsetAsync(c, 0, 64, st));
+  CK(cudaMemsetAsync(ctx->d_count, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(ctx->d_bytes, 0, 8ull * B, st));
+  CK(cudaMemsetAsync(ctx->d_stop, 0, 4ull * B, st));
+  k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, ctx->d_info, g, ctx->d_plan, ctx->index.d2, ctx->index.words,
+                                              ctx->d_tasks, c + 6, ctx->task_cap, ctx->d_safe, &g.ps->error); CKL();
+  SearchParams sp{};
+  sp.g = g; sp.plan = ctx->d_plan; sp.tasks = ctx->d_tasks; sp.n_tasks = c + 6; sp.task_cap = ctx->task_cap;
+  sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash;
+  sp.bytes = ctx->d_bytes; sp.stop = ctx->d_stop;
+  sp.d2 = ctx->index.d2; sp.d2_words = ctx->index.words; sp.cap = ctx->cfg.max_results;
+  sp.homo = ctx->cfg.homomorphism; sp.want_hash = 0; sp.error = &g.ps->error;
+  sp.q = ctx->d_q; sp.dq = ctx->d_dq; sp.qseq = ctx->d_qseq; sp.qcap = ctx->qcap;
+  sp.wait_limit_ns = 30ull * 1000000000ull;
+  sp.slot_limit_ns = 100ull * 1000000ull;
+  sp.task_limit_ns = 20ull * 1000000000ull;
+  sp.batch = B;
+  sp.sstat = ctx->d_sstat;
+  CK(cudaEventRecord(ctx->ev_start, st));
+  launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
+  CK(cudaEventRecord(ctx->ev_end, st));
+  CK(cudaEventSynchronize(ctx->ev_end));
+  CK(cudaEventElapsedTime(ms, ctx->ev_start, ctx->ev_end));
+  return check_device_error(ctx);
+}
+
+static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_t* out_w, uint32_t* out_b,
+                    float* out_ms) {
+  const uint32_t B = std::min<uint32_t>(n, ctx->bmax);
+  int rc = ensure_stream(ctx, B);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->d_stream, h_edges, B * sizeof(csm_update), cudaMemcpyHostToDevice, ctx->st));
+  k_tune_prep<<<blocks_for(B, 256), 256, 0, ctx->st>>>(ctx->d_stream, B, ctx->g, ctx->d_info); CKL();
+  int max_smem = 0;
+  CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->dev));
+  uint32_t best_w = 8, best_b = 1;
+  float best = 0, ms = 0;
+  bool have = false;
+  rc = tune_run(ctx, B, 8, 1, &ms);  // warm-up (caches, clocks)
+  if (rc) return rc;
+  for (uint32_t w : {4u, 8u, 16u}) {
+    const size_t smem = search_smem_bytes(ctx->nq, w) + 1024;  // + the runtime's per-block reserve
+    for (uint32_t b = 1; b * w <= 32; b++) {
+      if ((size_t)b * smem > (size_t)max_smem) break;
+      rc = tune_run(ctx, B, w, b, &ms);
+      if (rc) return rc;
+      if (!have || ms < best) { best = ms; best_w = w; best_b = b; have = true; }
+    }
+  }
+  ctx->cfg.warps_per_block = best_w;
+  ctx->cfg.blocks_per_sm = best_b;
+  *out_w = best_w; *out_b = best_b; *out_ms = best;
+  return CSM_OK;
+}
+
 // ------------------------------------------------------------ initial match
 
 // InitialMatching() (ParaCOSM/CSM/matching/GraphFlow/graphflow.cpp:268-284,
@@ -1116,6 +1198,22 @@ int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
     if (rc) return rc;
   }
   return initial_match(ctx, count);
+}
+
+int csm_gpu_autotune(csm_ctx* ctx, uint32_t n, const csm_update* edges, uint32_t* warps_per_block,
+                     uint32_t* blocks_per_sm, float* search_ms) {
+  if (!ctx || !edges || !warps_per_block || !blocks_per_sm || !search_ms) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
+  if (n == 0) return set_err(CSM_EINVAL, "empty sample");
+  CK(cudaSetDevice(ctx->dev));
+  int rc = ensure_batch_buffers(ctx);
+  if (rc) return rc;
+  if (ctx->owner) {
+    ctx->g = ctx->owner->g;
+    rc = stream_after(ctx->st, ctx->owner->st, ctx->ev_fork);
+    if (rc) return rc;
+  }
+  return autotune(ctx, n, edges, warps_per_block, blocks_per_sm, search_ms);
 }
 
 int csm_gpu_classify(csm_ctx* ctx, uint64_t n, const csm_update* ups, uint8_t* safe_out) {

@@ -108,6 +108,13 @@ class Engine:
         check(self.lib, self.lib.csm_gpu_initial_match(self.h, C.byref(c)))
         return int(c.value)
 
+    def autotune(self, sample: np.ndarray) -> dict:
+        """Picks the search launch shape from timings on sample edges (the graph is not modified)."""
+        u = np.ascontiguousarray(sample, dtype=UPDATE_DTYPE)
+        w, b, ms = C.c_uint32(), C.c_uint32(), C.c_float()
+        check(self.lib, self.lib.csm_gpu_autotune(self.h, len(u), _ptr(u), C.byref(w), C.byref(b), C.byref(ms)))
+        return {"warps_per_block": int(w.value), "blocks_per_sm": int(b.value), "sample_search_ms": float(ms.value)}
+
     # -- updates -------------------------------------------------------
     def classify(self, updates: np.ndarray) -> np.ndarray:
         u = np.ascontiguousarray(updates, dtype=UPDATE_DTYPE)

@@ -30,3 +30,13 @@ def test_unknown_algorithm_is_reported_like_the_reference():
     assert r.returncode == 1
     assert "----------- Loading graphs ------------" in r.stdout and "Unknown algorithm" in r.stdout
     assert "# vertices = 2048" in r.stdout
+
+
+def test_serve_tool_usage():
+    serve = ROOT / "paracosm_b200" / "_bin" / "csm_serve"
+    r = subprocess.run([str(serve), "-h"], capture_output=True, text=True)
+    assert r.returncode == 0
+    for opt in ("-w", "--rate", "--max-batch", "--budget-gb", "--arrive-every", "--out"):
+        assert opt in r.stderr
+    r = subprocess.run([str(serve)], capture_output=True, text=True)
+    assert r.returncode == 2
