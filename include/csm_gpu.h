@@ -79,8 +79,13 @@ typedef struct csm_cfg {
   uint32_t warps_per_block;   /* search kernel tuning; 0 = autotuned */
   uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
   uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */
-  uint32_t reserved[7];
+  int32_t graphs;             /* CSM_GRAPHS_*: replay each batch's launch sequence as a CUDA graph */
+  uint32_t reserved[6];
 } csm_cfg;
+
+#define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */
+#define CSM_GRAPHS_ON 1       /* capture a batch's launch sequence once per batch size and replay it
+                                 (search times are then not split out in csm_stats.search_ms) */
 
 /* Same 16-byte layout as the reference's InsertUnit fields
  * (ParaCOSM/CSM/utils/types.h:34-42). */

@@ -61,7 +61,8 @@ class CsmCfg(C.Structure):
         ("warps_per_block", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
         ("vertex_headroom", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("graphs", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

@@ -122,6 +122,22 @@ struct csm_ctx {
   csm_ctx* owner = nullptr;
   std::vector<csm_ctx*> attached;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // CUDA-graph replay of the batch launch sequence (owner only): one graph
+  // per batch size, rebuilt when the query set, the vertex count or the
+  // launch shape changes.  Batches read their updates from d_gups and write
+  // results to d_gres (one staging array per query), copied out after replay.
+  struct GraphEntry {
+    uint32_t B;
+    uint64_t version;
+    cudaGraphExec_t exec;
+    std::vector<uint64_t> launches;  // per query (owner, then attached)
+  };
+  std::vector<GraphEntry> graphs;
+  uint64_t graph_version = 1, graph_replays = 0;
+  bool capturing = false;
+  csm_update* d_gups = nullptr;
+  csm_result* d_gres = nullptr;
+  csm_update* d_gpad = nullptr;  // padding records: self loops, which are invalid and change nothing
 };
 
 namespace csm {
@@ -249,6 +265,14 @@ static int ensure_batch_buffers(csm_ctx* ctx) {
   AL(ctx->d_count, 8ull * B); AL(ctx->d_hash, 8ull * B); AL(ctx->d_bytes, 8ull * B);
   AL(ctx->d_stop, 4ull * B); AL(ctx->d_safe, 4ull * B);
   AL(ctx->d_stamp, 64);
+  AL(ctx->d_gups, sizeof(csm_update) * (size_t)B);
+  AL(ctx->d_gres, sizeof(csm_result) * (size_t)B);
+  AL(ctx->d_gpad, sizeof(csm_update) * (size_t)B);
+  {
+    std::vector<csm_update> pad(B, csm_update{'e', 1, 0, 0, 0, 0});
+    CK(cudaMemcpyAsync(ctx->d_gpad, pad.data(), sizeof(csm_update) * (size_t)B, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
   ctx->qcap = 1u << 16;  // outstanding handed-over tasks never exceed the idle warps
   AL(ctx->d_q, sizeof(SearchQueue));
   AL(ctx->d_sstat, sizeof(SearchStats));
@@ -403,16 +427,20 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   sp.sstat = q->d_sstat;
   uint32_t warps, bps;
   search_shape(q, warps, bps);
-  if (q->sev_used == q->sev.size()) {
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
-    q->sev.emplace_back(a, b);
+  if (o->capturing) {  // replays are not timed per search
+    launch_search(sp, q->nq, (uint32_t)q->sm_count * bps, warps, st); CKL();
+  } else {
+    if (q->sev_used == q->sev.size()) {
+      cudaEvent_t a, b;
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      q->sev.emplace_back(a, b);
+    }
+    CK(cudaEventRecord(q->sev[q->sev_used].first, st));
+    launch_search(sp, q->nq, (uint32_t)q->sm_count * bps, warps, st); CKL();
+    CK(cudaEventRecord(q->sev[q->sev_used].second, st));
+    q->sev_used++;
   }
-  CK(cudaEventRecord(q->sev[q->sev_used].first, st));
-  launch_search(sp, q->nq, (uint32_t)q->sm_count * bps, warps, st); CKL();
-  CK(cudaEventRecord(q->sev[q->sev_used].second, st));
-  q->sev_used++;
   k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_info, q->d_count, q->d_hash, q->d_bytes,
                                                   q->d_safe, q->cfg.max_results, q->cfg.want_hash, out); CKL();
   k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_stamp, out); CKL();
@@ -473,7 +501,7 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
 static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_update& h, csm_result* out,
                              const std::vector<csm_result*>& out_q) {
   cudaStream_t st = ctx->st;
-  if (h.is_add && h.id1 < ctx->g.n_cap && h.id1 >= ctx->g.n) ctx->g.n = h.id1 + 1;
+  if (h.is_add && h.id1 < ctx->g.n_cap && h.id1 >= ctx->g.n) { ctx->g.n = h.id1 + 1; ctx->graph_version++; }
   k_vertex_update<<<1, 32, 0, st>>>(ups, 1, ctx->g, ctx->d_info); CKL();
   CK(cudaMemsetAsync(ctx->d_safe, 0xff, 4, st));
   k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, 0, 0, out); CKL();
@@ -494,6 +522,75 @@ static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_upda
     rc = stream_after(st, a->st, a->ev_join);
     if (rc) return rc;
   }
+  return CSM_OK;
+}
+
+// A batch of B edge updates through a CUDA graph of its launch sequence.
+// Batch sizes are rounded up to a power of two (at most max_batch) with
+// padding records, so that batches of varying size -- as a serving loop
+// forms them -- share a few graphs.
+static int run_edge_batch_graph(csm_ctx* ctx, const csm_update* ups, uint32_t B_real, csm_result* out,
+                                const std::vector<csm_result*>& out_q) {
+  cudaStream_t st = ctx->st;
+  uint32_t B = 1;
+  while (B < B_real) B <<= 1;
+  B = std::min<uint32_t>(B, ctx->bmax);
+  std::vector<csm_ctx*> all{ctx};
+  all.insert(all.end(), ctx->attached.begin(), ctx->attached.end());
+  csm_ctx::GraphEntry* ge = nullptr;
+  for (auto& e : ctx->graphs)
+    if (e.B == B && e.version == ctx->graph_version) { ge = &e; break; }
+  if (!ge) {
+    // drop graphs of an older version (at most one per power of two is kept)
+    for (size_t i = 0; i < ctx->graphs.size();) {
+      if (ctx->graphs[i].version != ctx->graph_version || ctx->graphs.size() >= 18) {
+        cudaGraphExecDestroy(ctx->graphs[i].exec);
+        ctx->graphs.erase(ctx->graphs.begin() + (long)i);
+      } else {
+        i++;
+      }
+    }
+    std::vector<uint64_t> l0;
+    for (csm_ctx* q : all) l0.push_back(q->launches);
+    const uint64_t batches0 = ctx->batches;
+    std::vector<csm_result*> stage_q;
+    for (csm_ctx* a : ctx->attached) stage_q.push_back(a->d_gres);
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    int rc = run_edge_batch(ctx, ctx->d_gups, B, ctx->d_gres, stage_q);
+    ctx->capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (ce != cudaSuccess) return set_err(CSM_ECUDA, "graph capture: %s", cudaGetErrorString(ce));
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return set_err(CSM_ECUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+    csm_ctx::GraphEntry e{B, ctx->graph_version, exec, {}};
+    for (size_t k = 0; k < all.size(); k++) {
+      e.launches.push_back(all[k]->launches - l0[k]);
+      all[k]->launches = l0[k];  // counted when the graph runs
+    }
+    ctx->batches = batches0;
+    for (csm_ctx* a : ctx->attached) a->batches -= 1;
+    ctx->graphs.push_back(e);
+    ge = &ctx->graphs.back();
+  }
+  CK(cudaMemcpyAsync(ctx->d_gups, ups, sizeof(csm_update) * (size_t)B_real, cudaMemcpyDeviceToDevice, st));
+  if (B > B_real)
+    CK(cudaMemcpyAsync(ctx->d_gups + B_real, ctx->d_gpad, sizeof(csm_update) * (size_t)(B - B_real),
+                       cudaMemcpyDeviceToDevice, st));
+  CK(cudaGraphLaunch(ge->exec, st));
+  CK(cudaMemcpyAsync(out, ctx->d_gres, sizeof(csm_result) * (size_t)B_real, cudaMemcpyDeviceToDevice, st));
+  for (size_t k = 0; k < ctx->attached.size(); k++)
+    CK(cudaMemcpyAsync(out_q[k], ctx->attached[k]->d_gres, sizeof(csm_result) * (size_t)B_real,
+                       cudaMemcpyDeviceToDevice, st));
+  for (size_t k = 0; k < all.size(); k++) {
+    all[k]->launches += ge->launches[k];
+    all[k]->batches++;
+  }
+  ctx->graph_replays++;
   return CSM_OK;
 }
 
@@ -541,7 +638,10 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
     }
     uint64_t j = i;
     while (j < n && j - i < B && h[j].type != 'v') j++;
-    rc = run_edge_batch(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i, out_q);
+    if (ctx->cfg.graphs == CSM_GRAPHS_ON)
+      rc = run_edge_batch_graph(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i, out_q);
+    else
+      rc = run_edge_batch(ctx, d_ups + i, (uint32_t)(j - i), ctx->d_results + i, out_q);
     if (rc) return rc;
     ctx->e_updates += j - i;
     for (csm_ctx* a : ctx->attached) a->e_updates += j - i;
@@ -730,6 +830,8 @@ static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_
   }
   ctx->cfg.warps_per_block = best_w;
   ctx->cfg.blocks_per_sm = best_b;
+  ctx->graph_version++;
+  if (ctx->owner) ctx->owner->graph_version++;
   *out_w = best_w; *out_b = best_b; *out_ms = best;
   return CSM_OK;
 }
@@ -1055,6 +1157,7 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
   a->seq_next = owner->seq_next;
   a->owner = owner;
   owner->attached.push_back(a);
+  owner->graph_version++;
   *out = a;
   return CSM_OK;
 }
@@ -1386,7 +1489,10 @@ void csm_gpu_destroy(csm_ctx* ctx) {
   if (ctx->owner) {  // an attached query leaves its owner's list
     auto& v = ctx->owner->attached;
     v.erase(std::remove(v.begin(), v.end(), ctx), v.end());
+    ctx->owner->graph_version++;
   }
+  for (auto& e : ctx->graphs) cudaGraphExecDestroy(e.exec);
+  ctx->graphs.clear();
   for (csm_ctx* a : ctx->attached) {  // attached queries lose their graph; their calls then fail
     cudaStreamSynchronize(a->st);
     a->owner = nullptr;

@@ -38,7 +38,8 @@ class Engine:
     def __init__(self, algorithm: str | int = "parallel_graphflow", *, max_results: int = 0, homo: bool = False,
                  mode: str = "batched", max_batch: int = 65536, want_hash: bool = False, device: int = 0,
                  deadline_ns: int = 0, hbm_budget_bytes: int = 0, warps_per_block: int = 0,
-                 blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0):
+                 blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0,
+                 graphs: bool = False):
         self.lib = load_library()
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -55,6 +56,7 @@ class Engine:
         cfg.warps_per_block = int(warps_per_block)
         cfg.blocks_per_sm = int(blocks_per_sm)
         cfg.vertex_headroom = int(vertex_headroom)
+        cfg.graphs = int(bool(graphs))
         self.cfg = cfg
         h = C.c_void_p()
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))

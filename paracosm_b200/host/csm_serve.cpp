@@ -2,7 +2,7 @@
 //
 //   csm_serve -w WORKLOAD_DIR [--queries N] [--rate R] [--max-batch B] [--budget-gb G]
 //             [--cap N] [--plugins symbi,turboflux,graphflow] [--arrive-every S]
-//             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--device D]
+//             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1] [--device D]
 //             [--out results.bin]
 //   csm_serve -d data -u stream -q query[:plugin[:cap[:arrive_s]]] [-q ...] [same options]
 //
@@ -49,7 +49,8 @@ void usage() {
   fprintf(stderr,
           "csm_serve -w DIR | -d data -u stream -q query[:plugin[:cap[:arrive_s]]]...\n"
           "  [--queries N] [--rate R] [--max-batch B] [--budget-gb G] [--cap N] [--plugins a,b,c]\n"
-          "  [--arrive-every S] [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--device D]\n"
+          "  [--arrive-every S] [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]\n"
+          "  [--device D]\n"
           "  [--out results.bin]\n");
 }
 
@@ -84,6 +85,7 @@ int main(int argc, char** argv) {
     else if (k == "--max-seconds") cfg.max_seconds = std::stod(val());
     else if (k == "--seed") cfg.seed = std::stoull(val());
     else if (k == "--hash") cfg.want_hash = std::stoi(val()) != 0;
+    else if (k == "--graphs") cfg.graphs = std::stoi(val()) != 0;
     else if (k == "--device") cfg.device = std::stoi(val());
     else if (k == "--out") out_path = val();
     else if (k == "-h" || k == "--help") { usage(); return 0; }

@@ -44,6 +44,7 @@ int serve(const EdgeList& data, const std::vector<Update>& stream, const std::ve
   c.max_batch = cfg.max_batch;
   c.want_hash = cfg.want_hash ? 1 : 0;
   c.device = cfg.device;
+  c.graphs = cfg.graphs ? CSM_GRAPHS_ON : CSM_GRAPHS_OFF;
   Ctx owner;
   int rc = csm_gpu_create(&c, &owner.h);
   if (rc) return fail(rc, err, "create");

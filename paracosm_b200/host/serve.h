@@ -41,6 +41,7 @@ struct ServeConfig {
   double rate = 1e5;                     // offered load: Poisson arrivals, updates per second
   uint64_t seed = 7;
   bool want_hash = false;
+  bool graphs = true;                    // replay each batch size's launch sequence as a CUDA graph
   double max_seconds = 0;                // stop admitting updates after this long (0: run the stream)
 };
 

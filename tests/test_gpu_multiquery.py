@@ -51,11 +51,12 @@ def _owner(w, **kw):
     return eng
 
 
+@pytest.mark.parametrize("graphs", [False, True])
 @pytest.mark.parametrize("max_batch", [65536, 333])
-def test_each_query_alone_and_in_the_mix(wl, max_batch):
+def test_each_query_alone_and_in_the_mix(wl, max_batch, graphs):
     s = wl.stream
     alone = [_alone(wl, i, s, max_batch=max_batch) for i in range(len(QUERIES))]
-    with _owner(wl, max_batch=max_batch) as own:
+    with _owner(wl, max_batch=max_batch, graphs=graphs) as own:
         att = [own.attach(*wl.queries[i], PLUGINS[i], max_results=CAPS[i], want_hash=True)
                for i in range(1, len(QUERIES))]
         first = own.submit(s)

@@ -47,21 +47,24 @@ def test_golden_batched(case, algo):
     assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"], cap)
 
 
+@pytest.mark.parametrize("graphs", [False, True])
 @pytest.mark.parametrize("case", golden_cases())
-def test_golden_plain_one_update_per_launch(case):
+def test_golden_plain_one_update_per_launch(case, graphs):
     g = load_golden(case)
     cap = g["params"]["max_results"] or 0
     res, stats = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], max_results=cap, mode="plain",
-                            homo=g["params"]["homo"])
+                            homo=g["params"]["homo"], graphs=graphs)
     x = g["exp"]
     assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"], cap)
     assert stats["batches"] == np.sum(g["stream"]["type"] == ord("e"))
 
 
+@pytest.mark.parametrize("graphs", [False, True])
 @pytest.mark.parametrize("max_batch", [2, 7, 64, 333])
-def test_batch_boundaries_do_not_change_results(max_batch):
+def test_batch_boundaries_do_not_change_results(max_batch, graphs):
     g = load_golden("mixed_2el")
-    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], max_batch=max_batch)
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], max_batch=max_batch, graphs=graphs,
+                        algo="parallel_symbi")
     x = g["exp"]
     assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"])
 
@@ -118,6 +121,25 @@ def test_insert_then_delete_gives_equal_positive_and_negative(gen_dir):
     res, _ = run_engine(qv, qe, w.vlabels, w.edges, np.concatenate([ins, dels]))
     assert np.array_equal(res["pos"][: len(ins)], res["neg"][len(ins):][::-1])
     assert np.array_equal(res["hash"][: len(ins)], res["hash"][len(ins):][::-1])
+
+
+def test_graph_replay_counts_launches_and_survives_vertex_updates():
+    vl = np.array([0, 1, 0, 1, 0, 1], dtype=np.uint32)
+    edges = np.array([(0, 1, 0), (1, 2, 0), (2, 3, 0), (3, 4, 0)], dtype=np.uint32)
+    qv = np.array([0, 1, 0], dtype=np.uint32)
+    qe = np.array([(0, 1, 0), (1, 2, 0)], dtype=np.uint32)
+    e = lambda a, b: (ord("e"), 1, 0, a, b, 0)  # noqa: E731
+    ups = np.array([e(4, 5), e(0, 5), (ord("v"), 1, 0, 6, 0, 0), e(6, 1), e(6, 3), e(2, 5)], dtype=UPDATE_DTYPE)
+    ref = pyoracle.run(qv, qe, vl, edges, ups)
+    for mode in ("plain", "batched"):
+        with Engine("parallel_symbi", mode=mode, max_batch=2, graphs=True, want_hash=True) as eng:
+            eng.set_query(qv, qe)
+            eng.load_graph(vl, edges)
+            eng.build_index()
+            l0 = eng.kernel_launches()
+            res = eng.run(ups)
+            assert eng.kernel_launches() > l0
+        assert_same(res, ref["pos"], ref["neg"], ref["hash"])
 
 
 def test_vertex_insertion_then_edges():

@@ -64,13 +64,14 @@ def run_serve(d, tmp_path, *args):
     return json.loads(r.stdout.strip().splitlines()[-1]), read_results(out)
 
 
-def test_results_alone_and_in_the_served_mix(wl, tmp_path):
+@pytest.mark.parametrize("graphs", ["0", "1"])
+def test_results_alone_and_in_the_served_mix(wl, tmp_path, graphs):
     d, w = wl
     cap = 2000
-    # 6000 updates at 40k/s: about 0.15 s of arrivals; the second half of the
-    # queries arrives while updates are being served
+    # 6000 updates at 40k/s: about 0.15 s of arrivals; the later queries
+    # arrive while updates are being served
     summary, res = run_serve(d, tmp_path, "--rate", "40000", "--cap", str(cap), "--arrive-every", "0.03",
-                             "--max-batch", "1024")
+                             "--max-batch", "1024", "--graphs", graphs)
     assert summary["updates"] == len(w.stream)
     assert summary["batches"] > 1 and summary["mean_batch"] < len(w.stream)
     assert summary["queries_admitted"] == len(QUERIES)
