@@ -53,6 +53,13 @@ CONFIGS = {
         "workload": "RMAT 2^19 V, avg deg 16, 8 vlabels Zipf(1.0), 2 elabels; 8-vertex sparse query; "
                     "edge stream 90% insert / 10% delete; max_results 1e6 per update",
     },
+    "c4": {
+        "preset": "c4", "algo": "parallel_symbi", "batch": 65536, "max_results": 1_000_000,
+        "min_updates": 200_000,
+        "workload": "C3 graph (RMAT 2^22 V, avg deg 28, 16 vlabels Zipf(1.2), 4 elabels); 64 standing queries of "
+                    "4-32 vertices, half sparse, half dense, round-robin over SymBi / TurboFlux / GraphFlow; "
+                    "Poisson edge stream 85% insert / 15% delete; 40 GB device-memory budget; max_results 1e6",
+    },
     "c1": {
         "preset": "c1", "algo": "parallel_graphflow", "batch": 2000, "max_results": 0, "min_updates": 2000,
         "workload": "RMAT 2^14 V, avg deg 8, 4 vlabels, 1 elabel; 6-vertex induced query; 2,000 insertions",
@@ -235,6 +242,49 @@ def run_reference_arm(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def serve_sweep(w, cfg, rates, seconds, *, n_queries, device=0, plugins=None, cap=None) -> list[dict]:
+    """Runs the serving loop (paracosm_b200/_bin/csm_serve) on the workload at each offered rate."""
+    exe = ROOT / "paracosm_b200" / "_bin" / "csm_serve"
+    out = []
+    for r in rates:
+        cmd = [str(exe), "-w", str(w.directory), "--queries", str(n_queries), "--rate", str(r),
+               "--max-seconds", str(seconds), "--max-batch", str(cfg["batch"]), "--device", str(device),
+               "--cap", str(cfg["max_results"] if cap is None else cap),
+               "--plugins", ",".join(plugins or [cfg["algo"]]), "--graphs", "1"]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+        if p.returncode != 0:
+            out.append({"offered_rate": r, "error": p.stderr[-300:]})
+            continue
+        d = json.loads(p.stdout.strip().splitlines()[-1])
+        d["wall_s"] = time.perf_counter() - t0
+        out.append(d)
+        log(f"serve rate {r:g}: sustained {d['sustained']:.0f} upd/s p50 {d['p50_us']:.0f} us "
+            f"p99 {d['p99_us']:.0f} us mean batch {d['mean_batch']:.0f}")
+    return out
+
+
+def run_serving_config(args, cfg):
+    """C4: 64 standing queries (sizes 4-32, half sparse, half dense, round-robin over the
+    three plugins) on the C3 graph, Poisson arrivals swept over offered loads, admission
+    against a 40 GB budget.  value = the highest sustained updates/s of the sweep."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = get_workload(cfg, cfg["min_updates"])
+    plugins = ["parallel_symbi", "parallel_turboflux", "parallel_graphflow"]
+    rates = [float(r) for r in (args.serve_rates or "1e4,1e5,1e6").split(",") if r]
+    sweep = serve_sweep(w, cfg, rates, args.serve_seconds, n_queries=64, plugins=plugins)
+    ok = [d for d in sweep if "sustained" in d]
+    best = max(ok, key=lambda d: d["sustained"]) if ok else None
+    line = {"metric": METRIC, "value": best["sustained"] if best else None, "unit": "updates/s", "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "batch": cfg["batch"], "max_results": cfg["max_results"]},
+            "p50_us": best["p50_us"] if best else None, "p99_us": best["p99_us"] if best else None,
+            "serving": sweep}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -248,6 +298,10 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=3000)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the search-shape autotuner")
+    ap.add_argument("--serve-rates", default="1e4,1e5,1e6",
+                    help="offered loads (updates/s) for the serving-loop leg; empty to skip")
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.algo:
@@ -256,6 +310,8 @@ def main():
         cfg["batch"] = args.batch
     if args.impl == "reference":
         return run_reference_arm(args, cfg)
+    if args.config == "c4":
+        return run_serving_config(args, cfg)
 
     import torch
     import torch.distributed as dist
@@ -284,6 +340,11 @@ def main():
     eng.load_graph(w.vlabels, w.edges)
     eng.build_index()
     log(f"engine ready in {time.perf_counter() - t0:.1f}s")
+    shape = None
+    if not args.no_tune:
+        t1 = time.perf_counter()
+        shape = eng.autotune(np.ascontiguousarray(stream[: min(B, 4096)]))
+        log(f"autotuned search shape {shape} in {time.perf_counter() - t1:.1f}s")
     d_stream = torch.from_numpy(stream[: (W + K) * B].view(np.uint8).copy()).to(f"cuda:{dev}")
     ext = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{dev}")
     res_dev = torch.empty(K * B * RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{dev}")
@@ -346,28 +407,41 @@ def main():
     plain = None
     if rank == 0 and args.plain_sample > 0:
         P = min(args.plain_sample, len(stream))
-        peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev)
-        peng.set_query(qv, qe)
-        peng.load_graph(w.vlabels, w.edges)
-        peng.build_index()
+        sample = np.ascontiguousarray(stream[:P])
         beng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev)
         beng.set_query(qv, qe)
         beng.load_graph(w.vlabels, w.edges)
         beng.build_index()
-        sample = np.ascontiguousarray(stream[:P])
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        pr = peng.run(sample)
-        plain_s = time.perf_counter() - t1
-        pst = peng.stats()
         br = beng.run(sample)
-        same = bool(np.array_equal(pr["pos"], br["pos"]) and np.array_equal(pr["neg"], br["neg"]) and
-                    np.array_equal(pr["status"], br["status"]))
-        plain = {"value": P / plain_s, "updates": P, "device_ms": pst["total_device_ms"],
-                 "p50_us": float(np.percentile(np.diff(np.concatenate([[0], pr["latency_ns"]])), 50)) / 1e3,
-                 "counts_equal_batched": same}
-        peng.close()
         beng.close()
+        forms = {}
+        for graphs in (True, False):
+            kw = {"warps_per_block": shape["warps_per_block"], "blocks_per_sm": shape["blocks_per_sm"]} if shape else {}
+            peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev, graphs=graphs, **kw)
+            peng.set_query(qv, qe)
+            peng.load_graph(w.vlabels, w.edges)
+            peng.build_index()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            pr = peng.run(sample)
+            plain_s = time.perf_counter() - t1
+            pst = peng.stats()
+            same = bool(np.array_equal(pr["pos"], br["pos"]) and np.array_equal(pr["neg"], br["neg"]) and
+                        np.array_equal(pr["status"], br["status"]))
+            forms[graphs] = {"value": P / plain_s, "updates": P, "device_ms": pst["total_device_ms"],
+                             "p50_us": float(np.percentile(pr["latency_ns"], 50)) / 1e3,
+                             "p99_us": float(np.percentile(pr["latency_ns"], 99)) / 1e3,
+                             "kernel_launches_per_update": pst["kernel_launches"] / P,
+                             "counts_equal_batched": same}
+            peng.close()
+        plain = dict(forms[True], form="one update per launch sequence, replayed as a CUDA graph")
+        plain["without_graphs"] = dict(forms[False], form="one update per launch sequence, launched from the host")
+
+    # ---- serving loop: Poisson arrivals admitted in continuous batches ----
+    serving = None
+    if rank == 0 and world == 1 and args.serve_rates:
+        serving = serve_sweep(w, cfg, [float(r) for r in args.serve_rates.split(",") if r], args.serve_seconds,
+                              n_queries=1, device=dev)
 
     # ---- CPU baseline: the reference compiled from its sources, bounded sample ----
     cpu, cpu_seq = None, None
@@ -381,10 +455,12 @@ def main():
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32", "data": "synthetic",
             "config": {"workload": cfg["workload"], "plugin": cfg["algo"], "batch": B, "updates_timed": K * B,
+                       "search_shape": shape,
                        "l2": "inputs larger than L2 (graph ~1.2 GB in HBM)", "max_results": cfg["max_results"]},
             "p50_us": float(np.percentile(lat, 50)) / 1e3, "p99_us": float(np.percentile(lat, 99)) / 1e3,
             "plain": plain,
             "batched_over_plain": (value / plain["value"]) if plain else None,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": B * 16,
                     "d2h_bytes_per_step": B * RESULT_DTYPE.itemsize},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
