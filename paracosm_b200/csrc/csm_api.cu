@@ -387,14 +387,13 @@ static int batch_mutate_insert(csm_ctx* ctx, const csm_update* ups, uint32_t B, 
   return CSM_OK;
 }
 
+// Launch shape of the search: the configured (or autotuned) one, else 8
+// warps per block and as many blocks per SM as can be resident.
 static void search_shape(const csm_ctx* q, uint32_t& warps, uint32_t& bps) {
   warps = q->cfg.warps_per_block ? q->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   bps = q->cfg.blocks_per_sm ? q->cfg.blocks_per_sm : 0;
-  if (!bps) {
-    const size_t smem = search_smem_bytes(q->nq, warps);
-    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
-  }
+  if (!bps) bps = std::max<uint32_t>(1, search_max_blocks(q->nq, warps));
 }
 
 // One standing query q over the owner o's union graph: index to the union
@@ -812,17 +811,14 @@ static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_
   if (rc) return rc;
   CK(cudaMemcpyAsync(ctx->d_stream, h_edges, B * sizeof(csm_update), cudaMemcpyHostToDevice, ctx->st));
   k_tune_prep<<<blocks_for(B, 256), 256, 0, ctx->st>>>(ctx->d_stream, B, ctx->g, ctx->d_info); CKL();
-  int max_smem = 0;
-  CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->dev));
   uint32_t best_w = 8, best_b = 1;
   float best = 0, ms = 0;
   bool have = false;
   rc = tune_run(ctx, B, 8, 1, &ms);  // warm-up (caches, clocks)
   if (rc) return rc;
   for (uint32_t w : {4u, 8u, 16u}) {
-    const size_t smem = search_smem_bytes(ctx->nq, w) + 1024;  // + the runtime's per-block reserve
-    for (uint32_t b = 1; b * w <= 32; b++) {
-      if ((size_t)b * smem > (size_t)max_smem) break;
+    const uint32_t bmax = search_max_blocks(ctx->nq, w);  // resident blocks per SM
+    for (uint32_t b = std::max<uint32_t>(1, bmax > 3 ? bmax - 3 : 1); b <= bmax; b++) {
       rc = tune_run(ctx, B, w, b, &ms);
       if (rc) return rc;
       if (!have || ms < best) { best = ms; best_w = w; best_b = b; have = true; }
@@ -913,13 +909,8 @@ static int initial_match(csm_ctx* ctx, uint64_t* out) {
   CK(cudaMemcpyAsync(&last_cnt, cnt + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const unsigned long long n_seeds = last_off + last_cnt;
-  uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
-  if (warps != 4 && warps != 8 && warps != 16) warps = 8;
-  uint32_t bps = ctx->cfg.blocks_per_sm ? ctx->cfg.blocks_per_sm : 0;
-  if (!bps) {
-    const size_t smem = search_smem_bytes(ctx->nq, warps);
-    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
-  }
+  uint32_t warps, bps;
+  search_shape(ctx, warps, bps);
   for (unsigned long long first = 0; first < n_seeds; first += ctx->bmax) {
     const uint32_t B = (uint32_t)std::min<unsigned long long>(ctx->bmax, n_seeds - first);
     unsigned int* c = ctx->d_cnt;

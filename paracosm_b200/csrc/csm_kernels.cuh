@@ -126,6 +126,7 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
                        uint32_t* safe, unsigned int* error);
 size_t search_smem_bytes(uint32_t n_q, uint32_t warps);
+uint32_t search_max_blocks(uint32_t n_q, uint32_t warps);
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,

@@ -84,6 +84,9 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
 
 // Full candidate check of data vertex x for position `pos` given the matched
 // prefix m[0 .. pos-1]; `dsel` is the back entry whose segment produced x.
+// The joins are done four back entries at a time: their segment bounds are
+// loaded together and their binary searches advance in lockstep, so each
+// round trip to L2 serves up to four searches instead of one.
 __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uint32_t* pool, const PlanAnchor* A,
                                                 uint32_t pos, uint32_t x, const uint32_t* m, uint32_t dsel,
                                                 int32_t t) {
@@ -94,15 +97,46 @@ __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uin
     }
   }
   if (p.d2 && !d2_bit(p.d2, p.d2_words, P.qv, x)) return false;
-  for (uint32_t b = 0; b < P.nb; b++) {
-    const uint32_t j = A->back_pos[P.boff + b], c = A->back_combo[P.boff + b];
-    const uint32_t v = m[j];
-    if (b != dsel) {
-      uint64_t lo, hi;
-      segment(p.g, v, c, lo, hi);
-      if (!contains_u32(pool, lo, hi, x)) return false;
+  for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
+    uint32_t v[4], c[4], lo[4], hi[4], end[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b = b0 + (uint32_t)i;
+      v[i] = 0; c[i] = 0; lo[i] = 0; hi[i] = 0; end[i] = 0;
+      if (b < P.nb) {
+        v[i] = m[A->back_pos[P.boff + b]];
+        c[i] = A->back_combo[P.boff + b];
+        if (b != dsel) {
+          uint64_t l, h;
+          segment(p.g, v[i], c[i], l, h);
+          lo[i] = (uint32_t)l; hi[i] = (uint32_t)h; end[i] = (uint32_t)h;
+        }
+      }
     }
-    if (!present_at(p.g, v, c, x, t)) return false;
+    // lower_bound of x in each segment, one probe per segment per round
+    for (;;) {
+      bool more = false;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        if (lo[i] < hi[i]) {
+          const uint32_t mid = (lo[i] + hi[i]) >> 1;
+          if (pool[mid] < x) lo[i] = mid + 1; else hi[i] = mid;
+          more = true;
+        }
+      }
+      if (!more) break;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b = b0 + (uint32_t)i;
+      if (b >= P.nb || b == dsel) continue;
+      if (lo[i] >= end[i] || pool[lo[i]] != x) return false;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (b0 + (uint32_t)i >= P.nb) continue;
+      if (!present_at(p.g, v[i], c[i], x, t)) return false;
+    }
   }
   return true;
 }
@@ -110,7 +144,7 @@ __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uin
 // Driver segment of position np for prefix m (the smallest union-graph back
 // segment); false if some back segment is empty at batch time t.  `bytes`
 // receives 4 B x the sizes at time t of all back segments: the algorithmic
-// bytes of expanding this node.
+// bytes of expanding this node.  Segment bounds are loaded four at a time.
 __device__ __forceinline__ bool pick_driver(const SearchParams& p, const PlanAnchor* A, uint32_t np,
                                             const uint32_t* m, int32_t t, uint32_t& dlo, uint32_t& dn,
                                             uint32_t& dsel, unsigned long long& bytes) {
@@ -118,15 +152,29 @@ __device__ __forceinline__ bool pick_driver(const SearchParams& p, const PlanAnc
   uint32_t best = 0xffffffffu;
   bool empty = false;
   unsigned long long b4 = 0;
-  for (uint32_t b = 0; b < P.nb; b++) {
-    const uint32_t j = A->back_pos[P.boff + b], c = A->back_combo[P.boff + b];
-    uint64_t lo, hi;
-    segment(p.g, m[j], c, lo, hi);
-    const uint32_t sz = (uint32_t)(hi - lo);
-    const uint32_t szt = seg_size_at(p.g, m[j], c, lo, hi, t);
-    b4 += 4ull * szt;
-    if (szt == 0) empty = true;
-    if (sz < best) { best = sz; dsel = b; dlo = (uint32_t)lo; }
+  for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
+    uint32_t v[4], c[4];
+    uint64_t lo[4], hi[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b = b0 + (uint32_t)i;
+      lo[i] = 0; hi[i] = 0; v[i] = 0; c[i] = 0;
+      if (b < P.nb) {
+        v[i] = m[A->back_pos[P.boff + b]];
+        c[i] = A->back_combo[P.boff + b];
+        segment(p.g, v[i], c[i], lo[i], hi[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b = b0 + (uint32_t)i;
+      if (b >= P.nb) continue;
+      const uint32_t sz = (uint32_t)(hi[i] - lo[i]);
+      const uint32_t szt = seg_size_at(p.g, v[i], c[i], lo[i], hi[i], t);
+      b4 += 4ull * szt;
+      if (szt == 0) empty = true;
+      if (sz < best) { best = sz; dsel = b; dlo = (uint32_t)lo[i]; }
+    }
   }
   dn = best;
   bytes = b4;
@@ -596,6 +644,30 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
     atomicAdd(&p.sstat->checks_hungry, acc.checks_hungry);
     atomicMax(&p.sstat->max_task_ns, max_task);
   }
+}
+
+// Blocks of the search kernel that can be resident on one SM for this query
+// size (registers, shared memory and warp slots), from the occupancy API.
+uint32_t search_max_blocks(uint32_t n_q, uint32_t warps) {
+  const size_t smem = search_smem_bytes(n_q, warps);
+  int nb = 0;
+  cudaError_t e = cudaSuccess;
+  switch (warps) {
+    case 4:
+      cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<4>, 4 * 32, smem);
+      break;
+    case 16:
+      cudaFuncSetAttribute(k_search<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<16>, 16 * 32, smem);
+      break;
+    default:
+      cudaFuncSetAttribute(k_search<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<8>, 8 * 32, smem);
+      break;
+  }
+  if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+  return (uint32_t)nb;
 }
 
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s) {
