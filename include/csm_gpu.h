@@ -67,15 +67,18 @@ typedef struct csm_cfg {
   int32_t algorithm;          /* CSM_ALGO_* */
   int32_t homomorphism;       /* != 0: drop the injectivity check (reference --homo) */
   uint64_t max_results;       /* per-update cap (reference --max-results); 0 = none */
-  uint64_t deadline_ns;       /* per-update time budget on the device; 0 = none */
+  uint64_t deadline_ns;       /* per-update time budget, counted on the device from the start of the
+                                 search launch that holds the update; past it the update stops and
+                                 reports CSM_ST_TIMED_OUT with its count so far; 0 = none */
   uint64_t hbm_budget_bytes;  /* device memory the context may hold; 0 = 90% of free */
   int32_t mode;               /* CSM_MODE_* */
   uint32_t max_batch;         /* updates per batch in CSM_MODE_BATCHED (<= 65536); 0 = 65536 */
   int32_t want_hash;          /* != 0: compute the per-update match-set hash */
   int32_t device;             /* CUDA device ordinal */
-  int32_t turboflux_compat;   /* != 0: reproduce the reference TurboFlux deletion count,
-                                 which ignores the anchor edge label
-                                 (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:975) */
+  int32_t turboflux_compat;   /* reserved: would reproduce the reference TurboFlux deletion
+                                 count, which ignores the anchor edge label
+                                 (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:975);
+                                 != 0 is refused with CSM_EUNSUPPORTED */
   uint32_t warps_per_block;   /* search kernel tuning; 0 = autotuned */
   uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
   uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */

@@ -424,6 +424,7 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   sp.task_limit_ns = 20ull * 1000000000ull;
   sp.batch = B;
   sp.sstat = q->d_sstat;
+  sp.deadline_ns = q->cfg.deadline_ns;
   uint32_t warps, bps;
   search_shape(q, warps, bps);
   if (o->capturing) {  // replays are not timed per search
@@ -441,7 +442,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
     q->sev_used++;
   }
   k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_info, q->d_count, q->d_hash, q->d_bytes,
-                                                  q->d_safe, q->cfg.max_results, q->cfg.want_hash, out); CKL();
+                                                  q->d_safe, q->d_stop, q->cfg.max_results, q->cfg.want_hash,
+                                                  out); CKL();
   k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_stamp, out); CKL();
   return CSM_OK;
 }
@@ -497,13 +499,75 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   return CSM_OK;
 }
 
+// Vertex deletion (Graph::RemoveVertex, ParaCOSM/CSM/graph/graph.cpp:51-56, and
+// the plugins' RemoveVertex, e.g. SymBi/symbi.cpp:992-1021): every incident
+// edge leaves both endpoint rows, every query's index follows, then the slot
+// loses its label.  No embeddings are counted, as in the reference.
+static int run_vertex_delete(csm_ctx* ctx, uint32_t v) {
+  cudaStream_t st = ctx->st;
+  DevGraph& g = ctx->g;
+  uint32_t deg = 0;
+  CK(cudaMemcpyAsync(&deg, g.dir + (size_t)v * (g.nc + 1) + g.nc, 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<csm_ctx*> all{ctx};
+  all.insert(all.end(), ctx->attached.begin(), ctx->attached.end());
+  if (deg) {
+    const uint32_t K = 2 * deg;
+    uint64_t *keys = nullptr, *keys2 = nullptr;
+    VRange* ranges = nullptr;
+    unsigned int* nr = nullptr;
+    void* tmp = nullptr;
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, keys2, (int)K, 0, (int)g.kb.total(), st));
+    int rc = ctx->mem.alloc((void**)&keys, 8ull * K);
+    if (!rc) rc = ctx->mem.alloc((void**)&keys2, 8ull * K);
+    if (!rc) rc = ctx->mem.alloc((void**)&ranges, sizeof(VRange) * (size_t)K);
+    if (!rc) rc = ctx->mem.alloc((void**)&nr, 16);
+    if (!rc) rc = ctx->mem.alloc(&tmp, tb);
+    auto release = [&]() {
+      ctx->mem.release(keys, 8ull * K); ctx->mem.release(keys2, 8ull * K);
+      ctx->mem.release(ranges, sizeof(VRange) * (size_t)K); ctx->mem.release(nr, 16); ctx->mem.release(tmp, tb);
+    };
+    if (rc) { release(); return rc; }
+    k_vdel_keys<<<blocks_for(deg, 256), 256, 0, st>>>(g, v, deg, keys); CKL();
+    CK(cub::DeviceRadixSort::SortKeys(tmp, tb, keys, keys2, (int)K, 0, (int)g.kb.total(), st));
+    CK(cudaMemsetAsync(nr, 0, 16, st));
+    k_ranges<<<blocks_for(K, 256), 256, 0, st>>>(keys2, K, g.kb, ranges, nr); CKL();
+    const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(K * 32ull, 256), (uint32_t)ctx->sm_count * 16);
+    k_mut_delete<<<mut_blocks, 256, 0, st>>>(ranges, nr, keys2, g); CKL();
+    for (csm_ctx* q : all) {
+      if (q != ctx) { q->g = g; rc = stream_after(q->st, st, ctx->ev_fork); }
+      if (!rc) rc = index_apply_edges(q->index, g, keys2, K, q->st, &q->launches);
+      if (!rc && q != ctx) rc = stream_after(st, q->st, q->ev_join);
+      if (rc) { release(); return rc; }
+    }
+    CK(cudaStreamSynchronize(st));
+    release();
+  }
+  CK(cudaMemsetAsync(g.vlabel + v, 0xff, 4, st));
+  const csm_update del{'v', 0, 0, v, 0, 0};
+  for (csm_ctx* q : all) {
+    int rc = 0;
+    if (q != ctx) { q->g = g; rc = stream_after(q->st, st, ctx->ev_fork); }
+    if (!rc) rc = index_vertex_update(q->index, g, del, q->st, &q->launches);
+    if (!rc && q != ctx) rc = stream_after(st, q->st, q->ev_join);
+    if (rc) return rc;
+  }
+  ctx->graph_version++;
+  return CSM_OK;
+}
+
 static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_update& h, csm_result* out,
                              const std::vector<csm_result*>& out_q) {
   cudaStream_t st = ctx->st;
   if (h.is_add && h.id1 < ctx->g.n_cap && h.id1 >= ctx->g.n) { ctx->g.n = h.id1 + 1; ctx->graph_version++; }
+  if (!h.is_add && h.id1 < ctx->g.n) {
+    int rc = run_vertex_delete(ctx, h.id1);
+    if (rc) return rc;
+  }
   k_vertex_update<<<1, 32, 0, st>>>(ups, 1, ctx->g, ctx->d_info); CKL();
   CK(cudaMemsetAsync(ctx->d_safe, 0xff, 4, st));
-  k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, 0, 0, out); CKL();
+  k_finalize<<<1, 32, 0, st>>>(1, ctx->d_info, ctx->d_count, ctx->d_hash, nullptr, nullptr, nullptr, 0, 0, out); CKL();
   int rc = index_vertex_update(ctx->index, ctx->g, h, st, &ctx->launches);
   if (rc) return rc;
   for (size_t k = 0; k < ctx->attached.size(); k++) {
@@ -511,7 +575,8 @@ static int run_vertex_update(csm_ctx* ctx, const csm_update* ups, const csm_upda
     a->g = ctx->g;
     rc = stream_after(a->st, st, ctx->ev_fork);
     if (rc) return rc;
-    k_finalize<<<1, 32, 0, a->st>>>(1, ctx->d_info, a->d_count, a->d_hash, nullptr, nullptr, 0, 0, out_q[k]);
+    k_finalize<<<1, 32, 0, a->st>>>(1, ctx->d_info, a->d_count, a->d_hash, nullptr, nullptr, nullptr, 0, 0,
+                                    out_q[k]);
     a->launches++;
     CK(cudaGetLastError());
     rc = index_vertex_update(a->index, ctx->g, h, a->st, &a->launches);
@@ -976,6 +1041,8 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   if (!cfg || !out) return set_err(CSM_EINVAL, "null argument");
   if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
+  if (cfg->turboflux_compat)
+    return set_err(CSM_EUNSUPPORTED, "turboflux_compat (the reference TurboFlux deletion count) is not implemented");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(CSM_ECUDA, "no CUDA device");
   if (cfg->device < 0 || cfg->device >= ndev) return set_err(CSM_EINVAL, "bad device %d", cfg->device);

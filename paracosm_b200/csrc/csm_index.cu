@@ -468,7 +468,7 @@ int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, u
 
 int index_vertex_update(IndexState& ix, const DevGraph& g, const csm_update& h, cudaStream_t st, uint64_t* launches) {
   if (!ix.active) return CSM_OK;
-  if (h.type != 'v' || !h.is_add || h.id1 >= g.n_cap) return CSM_OK;
+  if (h.type != 'v' || h.id1 >= g.n_cap) return CSM_OK;  // a new or a removed vertex: re-evaluate its flags
   k_ix_seed_vertex<<<1, 32, 0, st>>>(h.id1, ix.d_dag, ix.bits);
   (*launches)++;
   return index_launch_round(ix, g, st, launches, false);

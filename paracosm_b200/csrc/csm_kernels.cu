@@ -435,9 +435,23 @@ __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges,
   }
 }
 
+// Vertex deletion: the packed keys of every directed entry incident to v,
+// (v, combo, y) and (y, combo', v), for the deletion kernels.
+__global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= deg) return;
+  const uint32_t* pool = g.pools[g.ps->active];
+  const uint32_t* dirv = g.dir + (size_t)v * (g.nc + 1);
+  const uint32_t y = pool[g.row_off[v] + i];
+  const uint32_t c = combo_at(dirv, g.nc, i);
+  const uint32_t el = c % g.n_el;
+  keys[2 * i] = g.kb.pack(v, c, y);
+  keys[2 * i + 1] = g.kb.pack(y, g.vlabel[v] * g.n_el + el, v);
+}
+
 // Vertex insertion (Graph::AddVertex, ParaCOSM/CSM/graph/graph.cpp:23-49): sets
-// the label of an absent vertex slot.  Vertex deletion is flagged invalid by
-// the caller.
+// the label of an absent vertex slot.  A deletion of an id beyond the
+// vertex slots is invalid; other deletions are applied by the caller.
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
@@ -447,7 +461,7 @@ __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, U
   inf.v1 = u.id1; inf.v2 = 0; inf.label = u.label; inf.flags = 0;
   if (u.is_add && u.id1 < g.n_cap) {
     if (g.vlabel[u.id1] == kNone) g.vlabel[u.id1] = fold_vlabel(g, u.label);
-  } else {
+  } else if (u.is_add || u.id1 >= g.n) {
     inf.flags = UF_INVALID;
   }
   info[s] = inf;

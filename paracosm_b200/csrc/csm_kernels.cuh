@@ -45,6 +45,7 @@ __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges,
                              uint32_t* ins_dst, DevGraph g);
 __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
                              DevGraph g);
+__global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys);
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
 
 // ---- search (csm_search.cu) ----
@@ -121,6 +122,7 @@ struct SearchParams {
   unsigned long long task_limit_ns;  // one task (a guard: a correct walk always ends)
   uint32_t batch;             // updates in this batch (bound of task update indices)
   SearchStats* sstat;
+  unsigned long long deadline_ns;  // per-update time budget from the launch's start; 0 = none
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
@@ -130,7 +132,9 @@ uint32_t search_max_blocks(uint32_t n_q, uint32_t warps);
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
-                           uint64_t cap, int want_hash, csm_result* out);
+                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out);
+// stop[] values: 1 = the cap was reached, 2 = the deadline passed first
+constexpr unsigned int kStopCap = 1u, kStopDeadline = 2u;
 __global__ void k_classify(uint64_t n, const csm_update* ups, DevGraph g, const Plan* plan, uint8_t* safe);
 
 }  // namespace csm

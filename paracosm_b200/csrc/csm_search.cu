@@ -290,6 +290,14 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
   const unsigned long long t_start = global_ns();
   while (d >= 1) {
     ++iter;
+    if ((iter & 63) == 0 && p.deadline_ns) {
+      unsigned int late = 0;
+      if (lane == 0 && global_ns() - p.sstat->launch_t0 > p.deadline_ns) {
+        atomicCAS(const_cast<unsigned int*>(stop) + t, 0u, kStopDeadline);
+        late = 1;
+      }
+      if (__shfl_sync(0xffffffffu, late, 0)) break;
+    }
     if ((iter & 63) == 0) {
       unsigned int expired = (lane == 0) ? (global_ns() - t_start > p.task_limit_ns) : 0u;
       if (__shfl_sync(0xffffffffu, expired, 0)) {
@@ -397,7 +405,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
         if (lane == 0) {
           const unsigned long long old = atomicAdd(&p.count[t], acc.cnt);
           acc.cnt = 0;
-          if (old + c >= p.cap) { stop[t] = 1u; hit = 1; }
+          if (old + c >= p.cap) { stop[t] = kStopCap; hit = 1; }
         }
         if (__shfl_sync(0xffffffffu, hit, 0)) break;
       }
@@ -419,7 +427,7 @@ __device__ __forceinline__ void flush_acc(const SearchParams& p, uint32_t t, uin
   if (lane == 0) {
     if (acc.cnt) {
       const unsigned long long old = atomicAdd(&p.count[t], acc.cnt);
-      if (p.cap && old + acc.cnt >= p.cap) p.stop[t] = 1u;
+      if (p.cap && old + acc.cnt >= p.cap) p.stop[t] = kStopCap;
     }
     if (p.want_hash && acc.hash) atomicAdd(&p.hash[t], acc.hash);
     if (acc.bytes) atomicAdd(&p.bytes[t], acc.bytes);
@@ -557,6 +565,8 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
     if (ti >= ntask) break;
     const Task T = p.tasks[ti];
     const unsigned long long tb = global_ns();
+    if (lane == 0 && p.deadline_ns && tb - p.sstat->launch_t0 > p.deadline_ns)
+      atomicCAS(const_cast<unsigned int*>(stop) + T.upd, 0u, kStopDeadline);
     // stop flags change under our feet: one lane reads, the warp follows it
     const unsigned int stopped = __shfl_sync(0xffffffffu, lane == 0 ? stop[T.upd] : 0u, 0);
     if (!stopped) run_root(p, pool, lv, lane, T, acc);
@@ -691,7 +701,7 @@ void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_
 
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
-                           uint64_t cap, int want_hash, csm_result* out) {
+                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
@@ -704,6 +714,7 @@ __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long 
   } else {
     unsigned long long c = count[s];
     if (cap && c >= cap) { c = cap; r.status = CSM_ST_CAPPED; }
+    else if (stop && stop[s] == kStopDeadline) r.status = CSM_ST_TIMED_OUT;  // c is a lower bound
     if (u.flags & UF_ADD) r.pos = c; else r.neg = c;
     if (want_hash && r.status == CSM_ST_OK) r.hash = hash[s];
     r.work_bytes = (bytes ? bytes[s] : 0ull) + ((u.flags & UF_MUT) ? 16ull : 0ull);

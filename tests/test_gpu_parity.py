@@ -7,7 +7,7 @@ import pytest
 
 from conftest import golden_cases, load_golden
 from oracle import pyoracle
-from paracosm_b200 import ST_CAPPED, ST_INVALID, ST_OK, UPDATE_DTYPE, Engine, workload
+from paracosm_b200 import ST_CAPPED, ST_INVALID, ST_OK, ST_TIMED_OUT, UPDATE_DTYPE, Engine, workload
 
 pytestmark = pytest.mark.gpu
 
@@ -153,3 +153,63 @@ def test_vertex_insertion_then_edges():
     res, _ = run_engine(qv, qe, vl, edges, ups)
     assert_same(res, ref["pos"], ref["neg"], ref["hash"])
     assert res["pos"][1] > 0
+
+
+def test_vertex_deletion_drops_incident_edges_everywhere():
+    """Vertex deletion (the oracle restates Graph::RemoveVertex with the incident edges
+    removed from both endpoints): later updates see the vertex gone, and a re-added
+    vertex starts without edges."""
+    g = load_golden("dense_del")
+    s = g["stream"]
+    hub = int(np.bincount(g["e"][:, :2].ravel()).argmax())
+    vdel = np.array([(ord("v"), 0, 0, hub, 0, 0)], dtype=UPDATE_DTYPE)
+    vadd = np.array([(ord("v"), 1, 0, hub, 0, int(g["vl"][hub]))], dtype=UPDATE_DTYPE)
+    ups = np.concatenate([s[:100], vdel, s[100:200], vadd, s[200:]])
+    ref = pyoracle.run(g["qv"], g["qe"], g["vl"], g["e"], ups)
+    for algo in ALGOS:
+        for mode in ("batched", "plain"):
+            res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], ups, algo, mode=mode)
+            assert_same(res, ref["pos"], ref["neg"], ref["hash"])
+            assert np.array_equal(res["status"] == ST_INVALID, ref["status"] == pyoracle.ST_INVALID)
+    with Engine("parallel_symbi") as eng:
+        eng.set_query(g["qv"], g["qe"])
+        eng.load_graph(g["vl"], g["e"])
+        eng.build_index()
+        eng.run(ups)
+        ix = eng.index(len(g["vl"]))
+        want = pyoracle.index(g["qv"], g["qe"], g["vl"], g["e"], ups, algo="symbi")
+        assert np.array_equal(ix["d1"][:, :len(g["vl"])], want["d1"][:, :len(g["vl"])])
+        assert np.array_equal(ix["d2"][:, :len(g["vl"])], want["d2"][:, :len(g["vl"])])
+        assert eng.initial_match() == pyoracle.initial_count(g["qv"], g["qe"], g["vl"], g["e"], ups)
+
+
+@pytest.mark.parametrize("case", ["c1_small", "mixed_2el", "dense_del", "zipf_8q"])
+def test_work_bytes_follow_the_canonical_model(case):
+    """GraphFlow without a cap expands exactly the oracle's search-tree nodes, so the
+    per-update algorithmic bytes are equal."""
+    g = load_golden(case)
+    ref = pyoracle.run(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], homo=g["params"]["homo"])
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], "parallel_graphflow",
+                        homo=g["params"]["homo"])
+    assert np.array_equal(res["work_bytes"], ref["bytes"]), np.nonzero(res["work_bytes"] != ref["bytes"])[0][:10]
+
+
+def test_deadline_reports_timed_out_with_lower_bounds():
+    g = load_golden("capped")  # dense enough that every matching update runs many iterations
+    ref = pyoracle.run(g["qv"], g["qe"], g["vl"], g["e"], g["stream"])
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], "parallel_symbi", deadline_ns=1)
+    timed = res["status"] == ST_TIMED_OUT
+    assert timed.any()
+    assert np.all(res["pos"][timed] <= ref["pos"][timed]) and np.all(res["neg"][timed] <= ref["neg"][timed])
+    ok = res["status"] == ST_OK
+    assert np.array_equal(res["pos"][ok], ref["pos"][ok]) and np.array_equal(res["neg"][ok], ref["neg"][ok])
+    # a generous deadline changes nothing
+    res2, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], "parallel_symbi", deadline_ns=60 * 10**9)
+    assert_same(res2, ref["pos"], ref["neg"], ref["hash"])
+
+
+def test_turboflux_compat_is_refused():
+    from paracosm_b200._abi import CSM_EUNSUPPORTED, CsmError
+    with pytest.raises(CsmError) as e:
+        Engine("parallel_turboflux", turboflux_compat=True)
+    assert e.value.code == CSM_EUNSUPPORTED
