@@ -481,7 +481,7 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   unsigned int* c = ctx->d_cnt;
   DevGraph& g = ctx->g;
   const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
-  k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, g); CKL();
+  k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, ctx->d_ins_dst, g); CKL();
   for (csm_ctx* a : ctx->attached) {
     rc = stream_after(a->st, st, ctx->ev_fork);
     if (!rc) rc = index_apply_edges(a->index, g, ctx->d_del2, L, a->st, &a->launches);
@@ -534,7 +534,7 @@ static int run_vertex_delete(csm_ctx* ctx, uint32_t v) {
     CK(cudaMemsetAsync(nr, 0, 16, st));
     k_ranges<<<blocks_for(K, 256), 256, 0, st>>>(keys2, K, g.kb, ranges, nr); CKL();
     const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(K * 32ull, 256), (uint32_t)ctx->sm_count * 16);
-    k_mut_delete<<<mut_blocks, 256, 0, st>>>(ranges, nr, keys2, g); CKL();
+    k_mut_delete<<<mut_blocks, 256, 0, st>>>(ranges, nr, keys2, reinterpret_cast<uint32_t*>(keys), g); CKL();
     for (csm_ctx* q : all) {
       if (q != ctx) { q->g = g; rc = stream_after(q->st, st, ctx->ev_fork); }
       if (!rc) rc = index_apply_edges(q->index, g, keys2, K, q->st, &q->launches);
@@ -743,7 +743,7 @@ static int check_device_error(csm_ctx* ctx) {
   if (ps.error) {
     static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow",
                                   "search queue wait limit", "malformed donated task", "ring left undrained",
-                                  "task time guard"};
+                                  "task time guard", "row state"};
     char extra[256] = "";
     if (ctx->d_sstat) {
       SearchStats ss;
@@ -766,7 +766,7 @@ static int check_device_error(csm_ctx* ctx) {
     ps.error = 0;
     cudaMemcpy(ctx->g.ps, &ps, sizeof(PoolState), cudaMemcpyHostToDevice);
     reset_ring(ctx);
-    return set_err(CSM_EDEVICE, "device error %u (%s)%s", code, code < 8 ? names[code] : "?", extra);
+    return set_err(CSM_EDEVICE, "device error %u (%s)%s", code, code < 9 ? names[code] : "?", extra);
   }
   return CSM_OK;
 }

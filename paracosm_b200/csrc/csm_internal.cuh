@@ -71,7 +71,7 @@ struct PoolState {
   uint32_t pad;
 };
 enum : uint32_t { kErrNone = 0, kErrPoolFull = 1, kErrListOverflow = 2, kErrTaskOverflow = 3, kErrWaitTimeout = 4,
-                  kErrBadTask = 5, kErrRingState = 6, kErrTaskGuard = 7 };
+                  kErrBadTask = 5, kErrRingState = 6, kErrTaskGuard = 7, kErrRowState = 8 };
 
 // Device view of the dynamic CSR (pointers into device memory).
 struct DevGraph {

@@ -333,8 +333,38 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* a, uint32_t 
   return lo;
 }
 
-// One warp per vertex: merges the vertex's sorted insert list into its row,
-// in place (moving old entries right, back to front) or into a larger row.
+// Warp copies of n pool entries.  Each round reads 32 entries into registers
+// before any lane writes, so a move that overlaps its source is safe when
+// left moves run front to back and right moves back to front.
+__device__ __forceinline__ void warp_move_left(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
+                                               uint32_t lane) {
+  for (uint32_t b = 0; b < n; b += 32) {
+    const uint32_t i = b + lane;
+    uint32_t v = 0;
+    if (i < n) v = pool[src + i];
+    __syncwarp();
+    if (i < n) pool[dst + i] = v;
+    __syncwarp();
+  }
+}
+__device__ __forceinline__ void warp_move_right(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
+                                                uint32_t lane) {
+  for (uint32_t b = n; b > 0;) {
+    const uint32_t cnt = min(32u, b);
+    b -= cnt;
+    uint32_t v = 0;
+    if (lane < cnt) v = pool[src + b + lane];
+    __syncwarp();
+    if (lane < cnt) pool[dst + b + lane] = v;
+    __syncwarp();
+  }
+}
+
+// One warp per vertex: merges the vertex's sorted insert list into its row.
+// Insert j (sorted by combo, then id) goes to row position p_j (its
+// lower_bound in the old row); old entries in [p_j, p_{j+1}) then shift by
+// j + 1, so the row moves as k + 1 contiguous blocks -- in place (last block
+// first, back to front) or into a larger row elsewhere.
 __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
                              uint32_t* ins_dst, DevGraph g) {
   const uint32_t lane = threadIdx.x & 31;
@@ -363,32 +393,30 @@ __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges,
       dst_off = o;
     }
     if (fail) continue;
-    // 1. destinations of the inserted entries, from the old row
+    // 1. positions p_j in the old row
     for (uint32_t j = lane; j < k; j += 32) {
       const uint64_t key = ins_key[s + j];
       const uint32_t c = g.kb.c_of(key), y = g.kb.y_of(key);
-      const uint64_t p = lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
-      ins_dst[s + j] = (uint32_t)p + j;
+      ins_dst[s + j] = (uint32_t)lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
     }
     __syncwarp();
-    // 2. old entries, back to front
-    for (int64_t base = (int64_t)deg; base > 0; base -= 32) {
-      const int64_t i = base - 1 - lane;
-      uint32_t y = 0, dst = 0;
-      if (i >= 0) {
-        y = pool[off + i];
-        const uint32_t c = combo_at(dirx, g.nc, (uint32_t)i);
-        const uint32_t sh = lower_bound_u64(ins_key, s, s + k, g.kb.pack(x, c, y)) - s;
-        dst = (uint32_t)i + sh;
+    // 2. old entries, block by block
+    if (dst_off == off) {
+      for (int64_t j = (int64_t)k - 1; j >= 0; j--) {
+        const uint32_t a = ins_dst[s + j], b = (j + 1 < (int64_t)k) ? ins_dst[s + j + 1] : deg;
+        if (b > a) warp_move_right(pool, off + a, off + a + (uint64_t)j + 1, b - a, lane);
       }
-      __syncwarp();
-      if (i >= 0) pool[dst_off + dst] = y;
-      __syncwarp();
+    } else {
+      warp_move_left(pool, off, dst_off, k ? ins_dst[s] : deg, lane);  // different rows: no overlap
+      for (uint32_t j = 0; j < k; j++) {
+        const uint32_t a = ins_dst[s + j], b = (j + 1 < k) ? ins_dst[s + j + 1] : deg;
+        if (b > a) warp_move_left(pool, off + a, dst_off + a + j + 1, b - a, lane);
+      }
     }
     // 3. inserted entries
-    for (uint32_t j = lane; j < k; j += 32) pool[dst_off + ins_dst[s + j]] = g.kb.y_of(ins_key[s + j]);
+    for (uint32_t j = lane; j < k; j += 32) pool[dst_off + ins_dst[s + j] + j] = g.kb.y_of(ins_key[s + j]);
     __syncwarp();
-    // 4. directory
+    // 4. directory: a combo's segment starts after the inserts of smaller combos
     for (uint32_t c = lane; c <= g.nc; c += 32) {
       const uint32_t add = lower_bound_u64(ins_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;
       dirx[c] += add;
@@ -399,9 +427,11 @@ __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges,
 }
 
 // One warp per vertex: removes the vertex's sorted delete list from its row
-// in place (front to back).
+// in place.  Delete j sits at row position q_j; the old entries between q_j
+// and q_{j+1} move left by j + 1, blocks front to back.  `del_pos` is
+// scratch of the delete list's length.
 __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
-                             DevGraph g) {
+                             uint32_t* del_pos, DevGraph g) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nr = *n_ranges;
   uint32_t* pool = g.pools[g.ps->active];
@@ -411,21 +441,19 @@ __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges,
     uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
     const uint32_t deg = dirx[g.nc];
     const uint64_t off = g.row_off[x];
-    for (uint32_t base = 0; base < deg; base += 32) {
-      const uint32_t i = base + lane;
-      uint32_t y = 0, dst = 0;
-      bool keep = false;
-      if (i < deg) {
-        y = pool[off + i];
-        const uint32_t c = combo_at(dirx, g.nc, i);
-        const uint64_t key = g.kb.pack(x, c, y);
-        const uint32_t p = lower_bound_u64(del_key, s, s + k, key);
-        keep = !(p < s + k && del_key[p] == key);
-        dst = i - (p - s);
+    for (uint32_t j = lane; j < k; j += 32) {
+      const uint64_t key = del_key[s + j];
+      const uint32_t c = g.kb.c_of(key), y = g.kb.y_of(key);
+      del_pos[s + j] = (uint32_t)lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
+    }
+    __syncwarp();
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t a = del_pos[s + j] + 1, b = (j + 1 < k) ? del_pos[s + j + 1] : deg;
+      if (a < j + 1 || a > deg) {  // a deleted entry missing from its row: leave the row, report
+        if (lane == 0) atomicExch(&g.ps->error, kErrRowState);
+        break;
       }
-      __syncwarp();
-      if (keep) pool[off + dst] = y;
-      __syncwarp();
+      if (b > a) warp_move_left(pool, off + a, off + a - (j + 1), b - a, lane);
     }
     for (uint32_t c = lane; c <= g.nc; c += 32) {
       const uint32_t sub = lower_bound_u64(del_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;

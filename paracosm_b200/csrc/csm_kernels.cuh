@@ -44,7 +44,7 @@ __global__ void k_compact_finish(DevGraph g);
 __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
                              uint32_t* ins_dst, DevGraph g);
 __global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
-                             DevGraph g);
+                             uint32_t* del_pos, DevGraph g);
 __global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys);
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
 
