@@ -371,9 +371,9 @@ static int batch_mutate_insert(csm_ctx* ctx, const csm_update* ups, uint32_t B, 
   CK(cub::DeviceRadixSort::SortKeys(ctx->d_cub, tb, ctx->d_del, ctx->d_del2, (int)L, 0, end_bit, st));
   tb = ctx->cub_bytes;
   CK(cub::DeviceRadixSort::SortPairs(ctx->d_cub, tb, ctx->d_tk, ctx->d_tk2, ctx->d_ts, ctx->d_ts2, (int)L, 0, end_bit, st));
-  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_ins2, L, kb, ctx->d_rins, c + 3); CKL();
-  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_del2, L, kb, ctx->d_rdel, c + 4); CKL();
-  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_tk2, L, kb, ctx->d_rt, c + 5); CKL();
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_ins2, L, kb, ctx->d_rins, c + 3, g.dir, g.nc); CKL();
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_del2, L, kb, ctx->d_rdel, c + 4, g.dir, g.nc); CKL();
+  k_ranges<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_tk2, L, kb, ctx->d_rt, c + 5, g.dir, g.nc); CKL();
   g.t_key = ctx->d_tk2;
   g.t_span = reinterpret_cast<int2*>(ctx->d_ts2);
   k_temporal_set<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
@@ -383,7 +383,9 @@ static int batch_mutate_insert(csm_ctx* ctx, const csm_update* ups, uint32_t B, 
   k_compact_copy<<<ctx->sm_count * 4, 1024, 0, st>>>(g); CKL();
   k_compact_finish<<<1, 1, 0, st>>>(g); CKL();
   const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
-  k_mut_insert<<<mut_blocks, 256, 0, st>>>(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g); CKL();
+  launch_mut_insert(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g, mut_blocks, (uint32_t)ctx->sm_count * 2, st);
+  CKL();
+  ctx->launches++;
   return CSM_OK;
 }
 
@@ -481,7 +483,9 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   unsigned int* c = ctx->d_cnt;
   DevGraph& g = ctx->g;
   const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(L * 32ull, 256), (uint32_t)ctx->sm_count * 16);
-  k_mut_delete<<<mut_blocks, 256, 0, st>>>(ctx->d_rdel, c + 4, ctx->d_del2, ctx->d_ins_dst, g); CKL();
+  launch_mut_delete(ctx->d_rdel, c + 4, ctx->d_del2, ctx->d_ins_dst, g, mut_blocks, (uint32_t)ctx->sm_count * 2, st);
+  CKL();
+  ctx->launches++;
   for (csm_ctx* a : ctx->attached) {
     rc = stream_after(a->st, st, ctx->ev_fork);
     if (!rc) rc = index_apply_edges(a->index, g, ctx->d_del2, L, a->st, &a->launches);
@@ -532,9 +536,12 @@ static int run_vertex_delete(csm_ctx* ctx, uint32_t v) {
     k_vdel_keys<<<blocks_for(deg, 256), 256, 0, st>>>(g, v, deg, keys); CKL();
     CK(cub::DeviceRadixSort::SortKeys(tmp, tb, keys, keys2, (int)K, 0, (int)g.kb.total(), st));
     CK(cudaMemsetAsync(nr, 0, 16, st));
-    k_ranges<<<blocks_for(K, 256), 256, 0, st>>>(keys2, K, g.kb, ranges, nr); CKL();
+    k_ranges<<<blocks_for(K, 256), 256, 0, st>>>(keys2, K, g.kb, ranges, nr, g.dir, g.nc); CKL();
     const uint32_t mut_blocks = std::min<uint32_t>(blocks_for(K * 32ull, 256), (uint32_t)ctx->sm_count * 16);
-    k_mut_delete<<<mut_blocks, 256, 0, st>>>(ranges, nr, keys2, reinterpret_cast<uint32_t*>(keys), g); CKL();
+    launch_mut_delete(ranges, nr, keys2, reinterpret_cast<uint32_t*>(keys), g, mut_blocks, (uint32_t)ctx->sm_count * 2,
+                      st);
+    CKL();
+    ctx->launches++;
     for (csm_ctx* q : all) {
       if (q != ctx) { q->g = g; rc = stream_after(q->st, st, ctx->ev_fork); }
       if (!rc) rc = index_apply_edges(q->index, g, keys2, K, q->st, &q->launches);

@@ -219,8 +219,11 @@ __global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B
   }
 }
 
-// Appends one VRange per vertex run of a sorted packed-key list.
-__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges) {
+// Appends one VRange per vertex run of a sorted packed-key list.  pad = 1
+// marks a row longer than kBigRow entries before the batch: the mutation
+// kernels give such rows a whole block instead of a warp.
+__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges,
+                         const uint32_t* dir, uint32_t nc) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= cap) return;
   const uint64_t k = key[j];
@@ -230,7 +233,8 @@ __global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* 
   uint32_t t = j + 1;
   while (t < cap && kb.real(key[t]) && kb.x_of(key[t]) == x) t++;
   unsigned int i = atomicAdd(n_ranges, 1u);
-  ranges[i] = VRange{x, j, t - j, 0};
+  const uint32_t big = dir[(size_t)x * (nc + 1) + nc] > kBigRow ? 1u : 0u;
+  ranges[i] = VRange{x, j, t - j, big};
 }
 
 __global__ void k_temporal_set(const VRange* ranges, const unsigned int* n_ranges, DevGraph g) {
@@ -333,45 +337,62 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* a, uint32_t 
   return lo;
 }
 
-// Warp copies of n pool entries.  Each round reads 32 entries into registers
-// before any lane writes, so a move that overlaps its source is safe when
-// left moves run front to back and right moves back to front.
-__device__ __forceinline__ void warp_move_left(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
-                                               uint32_t lane) {
-  for (uint32_t b = 0; b < n; b += 32) {
+// Group copies of n pool entries by G threads (a warp or a block).  Each
+// round reads G entries into registers before any thread writes, so a move
+// that overlaps its source is safe when left moves run front to back and
+// right moves back to front.
+template <int G>
+__device__ __forceinline__ void group_sync() {
+  if (G == 32) __syncwarp(); else __syncthreads();
+}
+template <int G>
+__device__ __forceinline__ void group_move_left(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
+                                                uint32_t lane) {
+  for (uint32_t b = 0; b < n; b += G) {
     const uint32_t i = b + lane;
     uint32_t v = 0;
     if (i < n) v = pool[src + i];
-    __syncwarp();
+    group_sync<G>();
     if (i < n) pool[dst + i] = v;
-    __syncwarp();
+    group_sync<G>();
   }
 }
-__device__ __forceinline__ void warp_move_right(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
-                                                uint32_t lane) {
+template <int G>
+__device__ __forceinline__ void group_move_right(uint32_t* pool, uint64_t src, uint64_t dst, uint32_t n,
+                                                 uint32_t lane) {
   for (uint32_t b = n; b > 0;) {
-    const uint32_t cnt = min(32u, b);
+    const uint32_t cnt = min((uint32_t)G, b);
     b -= cnt;
     uint32_t v = 0;
     if (lane < cnt) v = pool[src + b + lane];
-    __syncwarp();
+    group_sync<G>();
     if (lane < cnt) pool[dst + b + lane] = v;
-    __syncwarp();
+    group_sync<G>();
   }
 }
 
-// One warp per vertex: merges the vertex's sorted insert list into its row.
+// Merges each vertex's sorted insert list into its row; G = 32: one warp per
+// row of at most kBigRow entries, G = blockDim: one block per longer row.
 // Insert j (sorted by combo, then id) goes to row position p_j (its
 // lower_bound in the old row); old entries in [p_j, p_{j+1}) then shift by
 // j + 1, so the row moves as k + 1 contiguous blocks -- in place (last block
 // first, back to front) or into a larger row elsewhere.
-__global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
-                             uint32_t* ins_dst, DevGraph g) {
-  const uint32_t lane = threadIdx.x & 31;
+template <int G>
+__global__ void k_mut_insert_g(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
+                               uint32_t* ins_dst, DevGraph g) {
+  const uint32_t lane = threadIdx.x % G;
+  const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t nr = *n_ranges;
   PoolState* ps = g.ps;
   uint32_t* pool = g.pools[ps->active];
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nr; w += (gridDim.x * blockDim.x) >> 5) {
+  __shared__ unsigned long long s_off[8];
+  for (uint32_t w = blockIdx.x * groups_per_block + threadIdx.x / G; w - threadIdx.x / G < nr;
+       w += gridDim.x * groups_per_block) {
+    // every thread of a block-sized group walks the same w; warps of a
+    // warp-sized group skip ranges of the other kind
+    const bool mine = w < nr && ranges[w].pad == (G == 32 ? 0u : 1u);
+    if (G == 32 && !mine) continue;
+    if (G != 32 && !mine) { __syncthreads(); continue; }
     const VRange r = ranges[w];
     const uint32_t x = r.x, s = r.start, k = r.count;
     uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
@@ -380,87 +401,107 @@ __global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges,
     const uint32_t new_deg = deg + k;
     uint64_t dst_off = off;
     uint32_t new_cap = 0;
-    bool fail = false;
     if (new_deg > g.row_cap[x]) {
       new_cap = grow_cap(new_deg);
-      unsigned long long o = 0;
       if (lane == 0) {
-        o = atomicAdd(&ps->top[ps->active], (unsigned long long)new_cap);
+        unsigned long long o = atomicAdd(&ps->top[ps->active], (unsigned long long)new_cap);
         if (o + new_cap > g.pool_cap) { atomicExch(&ps->error, kErrPoolFull); o = ~0ULL; }
+        s_off[threadIdx.x / G] = o;
       }
-      o = __shfl_sync(0xffffffffu, o, 0);
-      if (o == ~0ULL) fail = true;
-      dst_off = o;
+      group_sync<G>();
+      dst_off = s_off[threadIdx.x / G];
+      group_sync<G>();
+      if (dst_off == ~0ULL) continue;  // uniform across the group
     }
-    if (fail) continue;
     // 1. positions p_j in the old row
-    for (uint32_t j = lane; j < k; j += 32) {
+    for (uint32_t j = lane; j < k; j += G) {
       const uint64_t key = ins_key[s + j];
       const uint32_t c = g.kb.c_of(key), y = g.kb.y_of(key);
       ins_dst[s + j] = (uint32_t)lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
     }
-    __syncwarp();
+    group_sync<G>();
     // 2. old entries, block by block
     if (dst_off == off) {
       for (int64_t j = (int64_t)k - 1; j >= 0; j--) {
         const uint32_t a = ins_dst[s + j], b = (j + 1 < (int64_t)k) ? ins_dst[s + j + 1] : deg;
-        if (b > a) warp_move_right(pool, off + a, off + a + (uint64_t)j + 1, b - a, lane);
+        if (b > a) group_move_right<G>(pool, off + a, off + a + (uint64_t)j + 1, b - a, lane);
       }
     } else {
-      warp_move_left(pool, off, dst_off, k ? ins_dst[s] : deg, lane);  // different rows: no overlap
+      group_move_left<G>(pool, off, dst_off, ins_dst[s], lane);  // different rows: no overlap
       for (uint32_t j = 0; j < k; j++) {
         const uint32_t a = ins_dst[s + j], b = (j + 1 < k) ? ins_dst[s + j + 1] : deg;
-        if (b > a) warp_move_left(pool, off + a, dst_off + a + j + 1, b - a, lane);
+        if (b > a) group_move_left<G>(pool, off + a, dst_off + a + j + 1, b - a, lane);
       }
     }
     // 3. inserted entries
-    for (uint32_t j = lane; j < k; j += 32) pool[dst_off + ins_dst[s + j] + j] = g.kb.y_of(ins_key[s + j]);
-    __syncwarp();
+    for (uint32_t j = lane; j < k; j += G) pool[dst_off + ins_dst[s + j] + j] = g.kb.y_of(ins_key[s + j]);
+    group_sync<G>();
     // 4. directory: a combo's segment starts after the inserts of smaller combos
-    for (uint32_t c = lane; c <= g.nc; c += 32) {
+    for (uint32_t c = lane; c <= g.nc; c += G) {
       const uint32_t add = lower_bound_u64(ins_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;
       dirx[c] += add;
     }
     if (lane == 0 && new_cap) { g.row_off[x] = dst_off; g.row_cap[x] = new_cap; }
-    __syncwarp();
+    group_sync<G>();
   }
 }
 
-// One warp per vertex: removes the vertex's sorted delete list from its row
-// in place.  Delete j sits at row position q_j; the old entries between q_j
-// and q_{j+1} move left by j + 1, blocks front to back.  `del_pos` is
-// scratch of the delete list's length.
-__global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
-                             uint32_t* del_pos, DevGraph g) {
-  const uint32_t lane = threadIdx.x & 31;
+// Removes each vertex's sorted delete list from its row in place (G as
+// above).  Delete j sits at row position q_j; the old entries between q_j and
+// q_{j+1} move left by j + 1, blocks front to back.  `del_pos` is scratch of
+// the delete list's length.
+template <int G>
+__global__ void k_mut_delete_g(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
+                               uint32_t* del_pos, DevGraph g) {
+  const uint32_t lane = threadIdx.x % G;
+  const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t nr = *n_ranges;
   uint32_t* pool = g.pools[g.ps->active];
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nr; w += (gridDim.x * blockDim.x) >> 5) {
+  for (uint32_t w = blockIdx.x * groups_per_block + threadIdx.x / G; w - threadIdx.x / G < nr;
+       w += gridDim.x * groups_per_block) {
+    const bool mine = w < nr && ranges[w].pad == (G == 32 ? 0u : 1u);
+    if (G == 32 && !mine) continue;
+    if (G != 32 && !mine) { __syncthreads(); continue; }
     const VRange r = ranges[w];
     const uint32_t x = r.x, s = r.start, k = r.count;
     uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
     const uint32_t deg = dirx[g.nc];
     const uint64_t off = g.row_off[x];
-    for (uint32_t j = lane; j < k; j += 32) {
+    for (uint32_t j = lane; j < k; j += G) {
       const uint64_t key = del_key[s + j];
       const uint32_t c = g.kb.c_of(key), y = g.kb.y_of(key);
       del_pos[s + j] = (uint32_t)lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
     }
-    __syncwarp();
+    group_sync<G>();
     for (uint32_t j = 0; j < k; j++) {
       const uint32_t a = del_pos[s + j] + 1, b = (j + 1 < k) ? del_pos[s + j + 1] : deg;
       if (a < j + 1 || a > deg) {  // a deleted entry missing from its row: leave the row, report
         if (lane == 0) atomicExch(&g.ps->error, kErrRowState);
         break;
       }
-      if (b > a) warp_move_left(pool, off + a, off + a - (j + 1), b - a, lane);
+      if (b > a) group_move_left<G>(pool, off + a, off + a - (j + 1), b - a, lane);
     }
-    for (uint32_t c = lane; c <= g.nc; c += 32) {
+    for (uint32_t c = lane; c <= g.nc; c += G) {
       const uint32_t sub = lower_bound_u64(del_key, s, s + k, g.kb.pack(x, 0, 0) + ((uint64_t)c << g.kb.yb)) - s;
       dirx[c] -= sub;
     }
-    __syncwarp();
+    group_sync<G>();
   }
+}
+
+// Both row kinds of a batch: rows up to kBigRow entries by warps, longer rows
+// by 256-thread blocks.
+void launch_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
+                       uint32_t* ins_dst, const DevGraph& g, uint32_t warp_blocks, uint32_t big_blocks,
+                       cudaStream_t st) {
+  k_mut_insert_g<32><<<warp_blocks, 256, 0, st>>>(ranges, n_ranges, ins_key, ins_dst, g);
+  k_mut_insert_g<256><<<big_blocks, 256, 0, st>>>(ranges, n_ranges, ins_key, ins_dst, g);
+}
+void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
+                       uint32_t* del_pos, const DevGraph& g, uint32_t warp_blocks, uint32_t big_blocks,
+                       cudaStream_t st) {
+  k_mut_delete_g<32><<<warp_blocks, 256, 0, st>>>(ranges, n_ranges, del_key, del_pos, g);
+  k_mut_delete_g<256><<<big_blocks, 256, 0, st>>>(ranges, n_ranges, del_key, del_pos, g);
 }
 
 // Vertex deletion: the packed keys of every directed entry incident to v,

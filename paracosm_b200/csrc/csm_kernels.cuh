@@ -34,17 +34,21 @@ struct ResolveOut {
 };
 __global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B, DevGraph g,
                           const csm_update* ups, UpdInfo* info, ResolveOut out);
-__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges);
+constexpr uint32_t kBigRow = 4096;  // rows longer than this are mutated by a whole block
+__global__ void k_ranges(const uint64_t* key, uint32_t cap, KeyBits kb, VRange* ranges, unsigned int* n_ranges,
+                         const uint32_t* dir, uint32_t nc);
 __global__ void k_temporal_set(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
 __global__ void k_temporal_clear(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
 __global__ void k_reloc_need(const VRange* ranges, const unsigned int* n_ranges, DevGraph g);
 __global__ void k_compact_check(DevGraph g);
 __global__ void k_compact_copy(DevGraph g);
 __global__ void k_compact_finish(DevGraph g);
-__global__ void k_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
-                             uint32_t* ins_dst, DevGraph g);
-__global__ void k_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
-                             uint32_t* del_pos, DevGraph g);
+void launch_mut_insert(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* ins_key,
+                       uint32_t* ins_dst, const DevGraph& g, uint32_t warp_blocks, uint32_t big_blocks,
+                       cudaStream_t st);
+void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const uint64_t* del_key,
+                       uint32_t* del_pos, const DevGraph& g, uint32_t warp_blocks, uint32_t big_blocks,
+                       cudaStream_t st);
 __global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys);
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
 
