@@ -83,7 +83,12 @@ typedef struct csm_cfg {
   uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
   uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */
   int32_t graphs;             /* CSM_GRAPHS_*: replay each batch's launch sequence as a CUDA graph */
-  uint32_t reserved[6];
+  uint32_t shard_rank;        /* seed sharding across GPUs: this context searches only the root tasks */
+  uint32_t shard_count;       /* (update, anchor, orientation) with (update + 2 * anchor + orientation)
+                                 % shard_count == shard_rank; the per-update results of all shards sum
+                                 to the unsharded ones (counts capped at max_results after the sum).
+                                 shard_count 0 or 1: no sharding */
+  uint32_t reserved[4];
 } csm_cfg;
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */

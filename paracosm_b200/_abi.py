@@ -62,7 +62,9 @@ class CsmCfg(C.Structure):
         ("blocks_per_sm", C.c_uint32),
         ("vertex_headroom", C.c_uint32),
         ("graphs", C.c_int32),
-        ("reserved", C.c_uint32 * 6),
+        ("shard_rank", C.c_uint32),
+        ("shard_count", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 

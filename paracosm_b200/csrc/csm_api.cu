@@ -413,7 +413,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   int rc = index_apply_edges(q->index, g, o->d_ins2, L, st, &q->launches);
   if (rc) return rc;
   k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, o->d_info, g, q->d_plan, q->index.d2, q->index.words,
-                                              q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error); CKL();
+                                              q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error,
+                                              q->cfg.shard_rank, q->cfg.shard_count); CKL();
   SearchParams sp{};
   sp.g = g; sp.plan = q->d_plan; sp.tasks = q->d_tasks; sp.n_tasks = c + 6; sp.task_cap = q->task_cap;
   sp.task_next = c + 7; sp.info = o->d_info; sp.count = q->d_count; sp.hash = q->d_hash; sp.bytes = q->d_bytes;
@@ -445,7 +446,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   }
   k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_info, q->d_count, q->d_hash, q->d_bytes,
                                                   q->d_safe, q->d_stop, q->cfg.max_results, q->cfg.want_hash,
-                                                  out); CKL();
+                                                  out, (q->cfg.shard_count > 1 && q->cfg.shard_rank) ? 0u : 16u);
+  CKL();
   k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_stamp, out); CKL();
   return CSM_OK;
 }
@@ -927,10 +929,11 @@ __global__ void k_init_count(DevGraph g, uint32_t la, uint32_t combo, unsigned l
 
 // Seeds [first, first + B) of the entry enumeration: info and one task each.
 __global__ void k_init_fill(DevGraph g, uint32_t combo, uint32_t label, const unsigned long long* off,
-                            unsigned long long first, uint32_t B, UpdInfo* info, Task* tasks) {
+                            unsigned long long first, uint32_t B, uint32_t stride, uint32_t rank, UpdInfo* info,
+                            Task* tasks) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= B) return;
-  const unsigned long long e = first + i;
+  const unsigned long long e = (first + i) * stride + rank;  // this shard's seeds
   uint32_t lo = 0, hi = g.n_cap;  // last x with off[x] <= e
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) >> 1;
@@ -980,7 +983,11 @@ static int initial_match(csm_ctx* ctx, uint64_t* out) {
   CK(cudaMemcpyAsync(&last_off, off + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&last_cnt, cnt + (n_cap - 1), 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  const unsigned long long n_seeds = last_off + last_cnt;
+  const unsigned long long n_all = last_off + last_cnt;
+  // with seed sharding this context takes the seeds e = k * shard_count + shard_rank
+  const uint32_t stride = ctx->cfg.shard_count > 1 ? ctx->cfg.shard_count : 1u;
+  const uint32_t rank = stride > 1 ? ctx->cfg.shard_rank : 0u;
+  const unsigned long long n_seeds = n_all > rank ? (n_all - rank + stride - 1) / stride : 0ull;
   uint32_t warps, bps;
   search_shape(ctx, warps, bps);
   for (unsigned long long first = 0; first < n_seeds; first += ctx->bmax) {
@@ -991,7 +998,8 @@ static int initial_match(csm_ctx* ctx, uint64_t* out) {
     CK(cudaMemsetAsync(ctx->d_count, 0, 8ull * B, st));
     CK(cudaMemsetAsync(ctx->d_bytes, 0, 8ull * B, st));
     CK(cudaMemsetAsync(ctx->d_stop, 0, 4ull * B, st));
-    k_init_fill<<<blocks_for(B, 256), 256, 0, st>>>(g, combo, A.el, off, first, B, ctx->d_info, ctx->d_tasks); CKL();
+    k_init_fill<<<blocks_for(B, 256), 256, 0, st>>>(g, combo, A.el, off, first, B, stride, rank, ctx->d_info,
+                                                    ctx->d_tasks); CKL();
     SearchParams sp{};
     sp.g = g; sp.plan = ctx->d_plan; sp.tasks = ctx->d_tasks; sp.n_tasks = c + 6; sp.task_cap = ctx->task_cap;
     sp.task_next = c + 7; sp.info = ctx->d_info; sp.count = ctx->d_count; sp.hash = ctx->d_hash;
@@ -1048,6 +1056,8 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   if (!cfg || !out) return set_err(CSM_EINVAL, "null argument");
   if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
+  if (cfg->shard_count > 1 && cfg->shard_rank >= cfg->shard_count)
+    return set_err(CSM_EINVAL, "shard_rank %u outside shard_count %u", cfg->shard_rank, cfg->shard_count);
   if (cfg->turboflux_compat)
     return set_err(CSM_EUNSUPPORTED, "turboflux_compat (the reference TurboFlux deletion count) is not implemented");
   int ndev = 0;

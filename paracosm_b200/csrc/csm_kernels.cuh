@@ -130,13 +130,14 @@ struct SearchParams {
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
-                       uint32_t* safe, unsigned int* error);
+                       uint32_t* safe, unsigned int* error, uint32_t shard_rank = 0, uint32_t shard_count = 1);
 size_t search_smem_bytes(uint32_t n_q, uint32_t warps);
 uint32_t search_max_blocks(uint32_t n_q, uint32_t warps);
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
-                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out);
+                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out,
+                           uint32_t mut_bytes = 16);  // bytes of an applied mutation (0 on secondary shards)
 // stop[] values: 1 = the cap was reached, 2 = the deadline passed first
 constexpr unsigned int kStopCap = 1u, kStopDeadline = 2u;
 __global__ void k_classify(uint64_t n, const csm_update* ups, DevGraph g, const Plan* plan, uint8_t* safe);

@@ -45,7 +45,7 @@ __device__ __forceinline__ bool d2_bit(const uint64_t* d2, uint64_t words, uint3
 
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
-                       uint32_t* safe, unsigned int* error) {
+                       uint32_t* safe, unsigned int* error, uint32_t shard_rank, uint32_t shard_count) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
@@ -64,6 +64,7 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
         if (!(o ? o1 : o0)) continue;
         const uint32_t x = o ? u.v2 : u.v1, y = o ? u.v1 : u.v2;
         if (d2 && !(d2_bit(d2, d2_words, A->pos[0].qv, x) && d2_bit(d2, d2_words, A->pos[1].qv, y))) continue;
+        if (shard_count > 1 && (s + 2 * a + (uint32_t)o) % shard_count != shard_rank) continue;  // another GPU's
         unsigned int i = atomicAdd(n_tasks, 1u);
         if (i >= task_cap) { atomicExch(error, kErrTaskOverflow); continue; }
         tasks[i] = Task{s, (uint16_t)a, (uint8_t)o, 0};
@@ -701,7 +702,8 @@ void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_
 
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
-                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out) {
+                           const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out,
+                           uint32_t mut_bytes) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
@@ -717,7 +719,7 @@ __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long 
     else if (stop && stop[s] == kStopDeadline) r.status = CSM_ST_TIMED_OUT;  // c is a lower bound
     if (u.flags & UF_ADD) r.pos = c; else r.neg = c;
     if (want_hash && r.status == CSM_ST_OK) r.hash = hash[s];
-    r.work_bytes = (bytes ? bytes[s] : 0ull) + ((u.flags & UF_MUT) ? 16ull : 0ull);
+    r.work_bytes = (bytes ? bytes[s] : 0ull) + ((u.flags & UF_MUT) ? (unsigned long long)mut_bytes : 0ull);
   }
   out[s] = r;
 }

@@ -39,7 +39,7 @@ class Engine:
                  mode: str = "batched", max_batch: int = 65536, want_hash: bool = False, device: int = 0,
                  deadline_ns: int = 0, hbm_budget_bytes: int = 0, warps_per_block: int = 0,
                  blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0,
-                 graphs: bool = False):
+                 graphs: bool = False, shard_rank: int = 0, shard_count: int = 1):
         self.lib = load_library()
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -57,6 +57,8 @@ class Engine:
         cfg.blocks_per_sm = int(blocks_per_sm)
         cfg.vertex_headroom = int(vertex_headroom)
         cfg.graphs = int(bool(graphs))
+        cfg.shard_rank = int(shard_rank)
+        cfg.shard_count = int(shard_count)
         self.cfg = cfg
         h = C.c_void_p()
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))
