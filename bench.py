@@ -60,6 +60,14 @@ CONFIGS = {
                     "4-32 vertices, half sparse, half dense, round-robin over SymBi / TurboFlux / GraphFlow; "
                     "Poisson edge stream 85% insert / 15% delete; 40 GB device-memory budget; max_results 1e6",
     },
+    "c5": {
+        "preset": "c5", "algo": "parallel_symbi", "batch": 8192, "max_results": 1_000_000,
+        "min_updates": 500_000, "deadline_ns": 1_000_000_000,
+        "workload": "RMAT 2^24 V, avg deg 32 (268M edges), 32 vlabels Zipf(1.0), 4 elabels; 24- and 32-vertex "
+                    "queries (sparse and dense) as four standing queries on one graph, plugins SymBi / TurboFlux / "
+                    "GraphFlow round-robin (the CaLiG- and NewSP-style plugins are not built); 90/10 insert/delete "
+                    "stream; per update max_results 1e6 and a 1 s limit",
+    },
     "c1": {
         "preset": "c1", "algo": "parallel_graphflow", "batch": 2000, "max_results": 0, "min_updates": 2000,
         "workload": "RMAT 2^14 V, avg deg 8, 4 vlabels, 1 elabel; 6-vertex induced query; 2,000 insertions",
@@ -285,6 +293,64 @@ def run_serving_config(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_stress_config(args, cfg):
+    """C5: four large standing queries on one 2^24-vertex graph, batches of 8,192 updates, a
+    per-update cap of 1e6 and a 1 s limit.  value = updates/s over the timed batches;
+    success rate = share of (update, query) results that are neither CAPPED nor TIMED_OUT."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch  # noqa: F401  (CUDA context order as in the main path)
+
+    from paracosm_b200 import ST_CAPPED, ST_TIMED_OUT, Engine
+    B, W, K = cfg["batch"], args.warmup, args.steps
+    w = get_workload(cfg, max(cfg["min_updates"], (W + K) * B))
+    plugins = ["parallel_symbi", "parallel_turboflux", "parallel_graphflow"]
+    t0 = time.perf_counter()
+    own = Engine(plugins[0], max_results=cfg["max_results"], max_batch=B, deadline_ns=cfg["deadline_ns"],
+                 graphs=True)
+    qv0, qe0 = w.queries[0]
+    own.set_query(qv0, qe0)
+    vls = np.concatenate([q[0] for q in w.queries])
+    els = np.concatenate([q[1][:, 2] for q in w.queries])
+    own.reserve_labels(np.unique(vls), np.unique(els))
+    own.load_graph(w.vlabels, w.edges)
+    own.build_index()
+    att = [own.attach(*w.queries[i], plugins[i % 3], max_results=cfg["max_results"]) for i in range(1, len(w.queries))]
+    log(f"engine with {len(w.queries)} queries ready in {time.perf_counter() - t0:.1f}s")
+    for i in range(W):
+        own.run(w.stream[i * B:(i + 1) * B])
+    t1 = time.perf_counter()
+    res = [[] for _ in range(len(w.queries))]
+    for k in range(K):
+        chunk = w.stream[(W + k) * B:(W + k + 1) * B]
+        first = own.submit(chunk)
+        own.wait()
+        res[0].append(own.results(first, len(chunk)))
+        for i, a in enumerate(att):
+            res[i + 1].append(a.results(first, len(chunk)))
+    secs = time.perf_counter() - t1
+    per_q = []
+    for i, rs in enumerate(res):
+        r = np.concatenate(rs)
+        bad = (r["status"] == ST_CAPPED) | (r["status"] == ST_TIMED_OUT)
+        per_q.append({"query": i, "vertices": int(len(w.queries[i][0])), "edges": int(len(w.queries[i][1])),
+                      "plugin": plugins[i % 3], "success_rate": float(1 - bad.mean()),
+                      "capped": int((r["status"] == ST_CAPPED).sum()),
+                      "timed_out": int((r["status"] == ST_TIMED_OUT).sum()),
+                      "p50_us": float(np.percentile(r["latency_ns"], 50)) / 1e3,
+                      "p99_us": float(np.percentile(r["latency_ns"], 99)) / 1e3})
+    allr = np.concatenate([np.concatenate(rs) for rs in res])
+    bad = (allr["status"] == ST_CAPPED) | (allr["status"] == ST_TIMED_OUT)
+    line = {"metric": METRIC, "value": K * B / secs, "unit": "updates/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "batch": B, "max_results": cfg["max_results"],
+                       "deadline_ns": cfg["deadline_ns"], "timing": "host wall clock around submit + results"},
+            "success_rate": float(1 - bad.mean()), "queries": per_q}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,6 +378,8 @@ def main():
         return run_reference_arm(args, cfg)
     if args.config == "c4":
         return run_serving_config(args, cfg)
+    if args.config == "c5":
+        return run_stress_config(args, cfg)
 
     import torch
     import torch.distributed as dist
