@@ -396,11 +396,11 @@ def main():
     torch.cuda.set_device(local)
     dev = local
     B, W, K, KE = cfg["batch"], args.warmup, args.steps, args.e2e_steps
-    n_updates = max(cfg["min_updates"], (W + K + KE) * B)
+    n_updates = max(cfg["min_updates"], (W + max(K, KE)) * B)
     w = get_workload(cfg, n_updates)
     qv, qe = w.queries[0]
     stream = w.stream
-    assert len(stream) >= (W + K + KE) * B
+    assert len(stream) >= (W + max(K, KE)) * B
 
     # ---- batched engine, inputs resident in HBM ----
     t0 = time.perf_counter()
@@ -461,8 +461,23 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = (work / 1e9) / (search_ms / 1e3) if search_ms > 0 else 0.0
 
-    # ---- e2e through the C ABI with pinned host buffers ----
-    host = torch.from_numpy(stream[(W + K) * B:(W + K + KE) * B].view(np.uint8).copy()).pin_memory()
+    eng.close()
+
+    # ---- e2e through the C ABI with pinned host buffers: a second engine from the
+    # same initial graph replays the warm-up batches, then takes the first KE timed
+    # batches of the stream from host memory (the same updates as the device-resident
+    # timed region starts with) ----
+    kw = {k: shape[k] for k in ("warps_per_block", "blocks_per_sm", "donate_every", "split_deep")} if shape else {}
+    eng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev,
+                 shard_rank=rank if world > 1 else 0, shard_count=world, **kw)
+    eng.set_query(qv, qe)
+    eng.load_graph(w.vlabels, w.edges)
+    eng.build_index()
+    ext = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{dev}")
+    for i in range(W):
+        eng.submit_device(d_stream.data_ptr() + i * B * 16, B)
+        eng.wait()
+    host = torch.from_numpy(stream[W * B:(W + KE) * B].view(np.uint8).copy()).pin_memory()
     e2e_ms = 0.0
     for k in range(KE):
         torch.cuda.synchronize()
@@ -498,7 +513,7 @@ def main():
         beng.close()
         forms = {}
         for graphs in (True, False):
-            kw = {"warps_per_block": shape["warps_per_block"], "blocks_per_sm": shape["blocks_per_sm"]} if shape else {}
+            kw = {k: shape[k] for k in ("warps_per_block", "blocks_per_sm", "donate_every", "split_deep")} if shape else {}
             peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev, graphs=graphs, **kw)
             peng.set_query(qv, qe)
             peng.load_graph(w.vlabels, w.edges)

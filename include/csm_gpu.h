@@ -88,7 +88,9 @@ typedef struct csm_cfg {
                                  % shard_count == shard_rank; the per-update results of all shards sum
                                  to the unsharded ones (counts capped at max_results after the sum).
                                  shard_count 0 or 1: no sharding */
-  uint32_t reserved[4];
+  uint32_t donate_every;      /* search hand-over check interval in steps (power of two); 0 = autotuned / 4 */
+  uint32_t split_deep;        /* smallest driver range split deep in the search tree; 0 = autotuned / 64 */
+  uint32_t reserved[2];
 } csm_cfg;
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */
@@ -188,13 +190,16 @@ int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count);
 /* Autotuner: times the search on n sample edges (host memory, type 'e'
  * records; searched as insertions into the current graph, which is not
  * modified) for every launch shape the SM admits -- warps per block x
- * resident blocks per SM -- and keeps the fastest for this context's later
- * searches.  Reports the shape and its search time on the sample.  The
+ * resident blocks per SM -- then for a few hand-over settings (check
+ * interval, smallest split range), and keeps the fastest for this context's
+ * later searches (a setting replaces the default only when it is at least 5 %
+ * faster).  Reports the choice (0 = the default hand-over setting) and its
+ * search time on the sample.  The
  * reference tunes its CPU thread count instead (--auto-tuning,
  * ParaCOSM/CSM/matching/Parallel_TurboFlux/parallel_turboflux.cpp); there is
  * no counterpart entry point. */
 int csm_gpu_autotune(csm_ctx* ctx, uint32_t n, const csm_update* edges, uint32_t* warps_per_block,
-                     uint32_t* blocks_per_sm, float* search_ms);
+                     uint32_t* blocks_per_sm, uint32_t* donate_every, uint32_t* split_deep, float* search_ms);
 
 /* Classify(v1, v2, label) for n updates: safe_out[i] = 1 when no query edge
  * matches the label triple (L(v1), L(v2), label) in either orientation

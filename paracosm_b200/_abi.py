@@ -64,7 +64,9 @@ class CsmCfg(C.Structure):
         ("graphs", C.c_int32),
         ("shard_rank", C.c_uint32),
         ("shard_count", C.c_uint32),
-        ("reserved", C.c_uint32 * 4),
+        ("donate_every", C.c_uint32),
+        ("split_deep", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 
@@ -105,7 +107,8 @@ _SIGNATURES = [
     ("csm_gpu_build_index", C.c_int, [C.c_void_p]),
     ("csm_gpu_initial_match", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("csm_gpu_autotune", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32),
-                                   C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
+                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_float)]),
     ("csm_gpu_classify", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("csm_gpu_submit", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
     ("csm_gpu_submit_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),

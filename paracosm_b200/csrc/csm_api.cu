@@ -428,6 +428,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   sp.batch = B;
   sp.sstat = q->d_sstat;
   sp.deadline_ns = q->cfg.deadline_ns;
+  sp.donate_every = q->cfg.donate_every;
+  sp.split_deep = q->cfg.split_deep;
   uint32_t warps, bps;
   search_shape(q, warps, bps);
   if (o->capturing) {  // replays are not timed per search
@@ -848,7 +850,8 @@ __global__ void k_tune_prep(const csm_update* edges, uint32_t n, DevGraph g, Upd
   info[i] = inf;
 }
 
-static int tune_run(csm_ctx* ctx, uint32_t B, uint32_t warps, uint32_t bps, float* ms) {
+static int tune_run(csm_ctx* ctx, uint32_t B, uint32_t warps, uint32_t bps, float* ms, uint32_t donate_every = 0,
+                    uint32_t split_deep = 0) {
   cudaStream_t st = ctx->st;
   const DevGraph& g = ctx->g;
   unsigned int* c = ctx->d_cnt;
@@ -870,6 +873,8 @@ static int tune_run(csm_ctx* ctx, uint32_t B, uint32_t warps, uint32_t bps, floa
   sp.task_limit_ns = 20ull * 1000000000ull;
   sp.batch = B;
   sp.sstat = ctx->d_sstat;
+  sp.donate_every = donate_every;
+  sp.split_deep = split_deep;
   CK(cudaEventRecord(ctx->ev_start, st));
   launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
   CK(cudaEventRecord(ctx->ev_end, st));
@@ -905,6 +910,17 @@ static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_
       if (ms < best && ms < 0.95f * def_ms) { best = ms; best_w = w; best_b = b; }
     }
   }
+  // hand-over settings for the chosen shape, against the default (4, 64)
+  uint32_t best_every = 0, best_split = 0;
+  const float shape_ms = best;
+  static const uint32_t kHandOver[4][2] = {{2u, 32u}, {8u, 128u}, {4u, 16u}, {16u, 256u}};
+  for (const auto& cand : kHandOver) {
+    rc = tune_run(ctx, B, best_w, best_b, &ms, cand[0], cand[1]);
+    if (rc) return rc;
+    if (ms < best && ms < 0.95f * shape_ms) { best = ms; best_every = cand[0]; best_split = cand[1]; }
+  }
+  ctx->cfg.donate_every = best_every;
+  ctx->cfg.split_deep = best_split;
   ctx->cfg.warps_per_block = best_w;
   ctx->cfg.blocks_per_sm = best_b;
   ctx->graph_version++;
@@ -1386,8 +1402,9 @@ int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {
 }
 
 int csm_gpu_autotune(csm_ctx* ctx, uint32_t n, const csm_update* edges, uint32_t* warps_per_block,
-                     uint32_t* blocks_per_sm, float* search_ms) {
-  if (!ctx || !edges || !warps_per_block || !blocks_per_sm || !search_ms) return set_err(CSM_EINVAL, "null argument");
+                     uint32_t* blocks_per_sm, uint32_t* donate_every, uint32_t* split_deep, float* search_ms) {
+  if (!ctx || !edges || !warps_per_block || !blocks_per_sm || !donate_every || !split_deep || !search_ms)
+    return set_err(CSM_EINVAL, "null argument");
   if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
   if (n == 0) return set_err(CSM_EINVAL, "empty sample");
   CK(cudaSetDevice(ctx->dev));
@@ -1398,7 +1415,10 @@ int csm_gpu_autotune(csm_ctx* ctx, uint32_t n, const csm_update* edges, uint32_t
     rc = stream_after(ctx->st, ctx->owner->st, ctx->ev_fork);
     if (rc) return rc;
   }
-  return autotune(ctx, n, edges, warps_per_block, blocks_per_sm, search_ms);
+  rc = autotune(ctx, n, edges, warps_per_block, blocks_per_sm, search_ms);
+  *donate_every = ctx->cfg.donate_every;
+  *split_deep = ctx->cfg.split_deep;
+  return rc;
 }
 
 int csm_gpu_classify(csm_ctx* ctx, uint64_t n, const csm_update* ups, uint8_t* safe_out) {

@@ -127,6 +127,10 @@ struct SearchParams {
   uint32_t batch;             // updates in this batch (bound of task update indices)
   SearchStats* sstat;
   unsigned long long deadline_ns;  // per-update time budget from the launch's start; 0 = none
+  // hand-over tuning: busy warps look for idle ones every donate_every
+  // iterations (a power of two; 0 = 4) and split a driver range deep in the
+  // tree only when at least split_deep elements remain (0 = 64)
+  uint32_t donate_every, split_deep;
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,

@@ -209,7 +209,7 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
     const uint32_t cnt = lv[L].cnt, ce = lv[L].cur_e;
     if (ce >= cnt) continue;
     if (cnt - ce >= 2) { Ls = L; mode = 1; break; }
-    const uint32_t min_split = (L + 5 <= n) ? 2u : 64u;
+    const uint32_t min_split = (L + 5 <= n) ? 2u : (p.split_deep ? p.split_deep : 64u);
     if (lv[L].dn[ce] - lv[L].cur_k >= min_split) { Ls = L; mode = 2; break; }
   }
   if (!mode) {
@@ -322,7 +322,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       uint32_t st = (lane == 0) ? stop[t] : 0u;
       if (__shfl_sync(0xffffffffu, st, 0)) break;
     }
-    if ((iter & 3) == 0 && p.dq) {
+    if ((iter & (p.donate_every ? p.donate_every - 1 : 3u)) == 0 && p.dq) {
       uint32_t idle_now = (lane == 0) ? *(volatile unsigned int*)&p.q->hungry : 0u;
       idle_now = __shfl_sync(0xffffffffu, idle_now, 0);
       acc.checks++;

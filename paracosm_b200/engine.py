@@ -39,7 +39,8 @@ class Engine:
                  mode: str = "batched", max_batch: int = 65536, want_hash: bool = False, device: int = 0,
                  deadline_ns: int = 0, hbm_budget_bytes: int = 0, warps_per_block: int = 0,
                  blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0,
-                 graphs: bool = False, shard_rank: int = 0, shard_count: int = 1):
+                 graphs: bool = False, shard_rank: int = 0, shard_count: int = 1, donate_every: int = 0,
+                 split_deep: int = 0):
         self.lib = load_library()
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -59,6 +60,8 @@ class Engine:
         cfg.graphs = int(bool(graphs))
         cfg.shard_rank = int(shard_rank)
         cfg.shard_count = int(shard_count)
+        cfg.donate_every = int(donate_every)
+        cfg.split_deep = int(split_deep)
         self.cfg = cfg
         h = C.c_void_p()
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))
@@ -115,9 +118,11 @@ class Engine:
     def autotune(self, sample: np.ndarray) -> dict:
         """Picks the search launch shape from timings on sample edges (the graph is not modified)."""
         u = np.ascontiguousarray(sample, dtype=UPDATE_DTYPE)
-        w, b, ms = C.c_uint32(), C.c_uint32(), C.c_float()
-        check(self.lib, self.lib.csm_gpu_autotune(self.h, len(u), _ptr(u), C.byref(w), C.byref(b), C.byref(ms)))
-        return {"warps_per_block": int(w.value), "blocks_per_sm": int(b.value), "sample_search_ms": float(ms.value)}
+        w, b, de, sd, ms = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_float()
+        check(self.lib, self.lib.csm_gpu_autotune(self.h, len(u), _ptr(u), C.byref(w), C.byref(b), C.byref(de),
+                                                  C.byref(sd), C.byref(ms)))
+        return {"warps_per_block": int(w.value), "blocks_per_sm": int(b.value), "donate_every": int(de.value),
+                "split_deep": int(sd.value), "sample_search_ms": float(ms.value)}
 
     # -- updates -------------------------------------------------------
     def classify(self, updates: np.ndarray) -> np.ndarray:
