@@ -2,7 +2,8 @@
 //
 //   csm_serve -w WORKLOAD_DIR [--queries N] [--rate R] [--max-batch B] [--budget-gb G]
 //             [--cap N] [--plugins symbi,turboflux,graphflow] [--arrive-every S]
-//             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1] [--device D]
+//             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]
+//             [--deadline-ms MS] [--device D]
 //             [--out results.bin]
 //   csm_serve -d data -u stream -q query[:plugin[:cap[:arrive_s]]] [-q ...] [same options]
 //
@@ -50,7 +51,7 @@ void usage() {
           "csm_serve -w DIR | -d data -u stream -q query[:plugin[:cap[:arrive_s]]]...\n"
           "  [--queries N] [--rate R] [--max-batch B] [--budget-gb G] [--cap N] [--plugins a,b,c]\n"
           "  [--arrive-every S] [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]\n"
-          "  [--device D]\n"
+          "  [--deadline-ms MS] [--device D]\n"
           "  [--out results.bin]\n");
 }
 
@@ -86,6 +87,7 @@ int main(int argc, char** argv) {
     else if (k == "--seed") cfg.seed = std::stoull(val());
     else if (k == "--hash") cfg.want_hash = std::stoi(val()) != 0;
     else if (k == "--graphs") cfg.graphs = std::stoi(val()) != 0;
+    else if (k == "--deadline-ms") cfg.deadline_ns = (uint64_t)(std::stod(val()) * 1e6);
     else if (k == "--device") cfg.device = std::stoi(val());
     else if (k == "--out") out_path = val();
     else if (k == "-h" || k == "--help") { usage(); return 0; }
@@ -139,11 +141,12 @@ int main(int argc, char** argv) {
   printf("{\"offered_rate\": %.1f, \"sustained\": %.1f, \"updates\": %llu, \"elapsed_s\": %.4f, \"p50_us\": %.1f, "
          "\"p99_us\": %.1f, \"batches\": %llu, \"mean_batch\": %.1f, \"max_batch_seen\": %llu, "
          "\"queries\": %zu, \"queries_admitted\": %u, \"queries_refused\": %u, \"device_bytes\": %llu, "
-         "\"positive\": %llu, \"negative\": %llu, \"capped\": %llu}\n",
+         "\"positive\": %llu, \"negative\": %llu, \"capped\": %llu, \"success_rate\": %.6f}\n",
          cfg.rate, st.sustained, (unsigned long long)st.updates, st.elapsed_s, st.p50_us, st.p99_us,
          (unsigned long long)st.batches, st.mean_batch, (unsigned long long)st.max_batch_seen, queries.size(),
          st.queries_admitted, st.queries_refused, (unsigned long long)st.device_bytes, (unsigned long long)pos,
-         (unsigned long long)neg, (unsigned long long)capped);
+         (unsigned long long)neg, (unsigned long long)capped,
+         st.results ? 1.0 - (double)st.incomplete / (double)st.results : 1.0);
   if (!out_path.empty()) {
     FILE* f = fopen(out_path.c_str(), "wb");
     if (!f) { fprintf(stderr, "cannot write %s\n", out_path.c_str()); return 1; }

@@ -45,6 +45,7 @@ int serve(const EdgeList& data, const std::vector<Update>& stream, const std::ve
   c.want_hash = cfg.want_hash ? 1 : 0;
   c.device = cfg.device;
   c.graphs = cfg.graphs ? CSM_GRAPHS_ON : CSM_GRAPHS_OFF;
+  c.deadline_ns = cfg.deadline_ns;  // attached queries inherit it
   Ctx owner;
   int rc = csm_gpu_create(&c, &owner.h);
   if (rc) return fail(rc, err, "create");
@@ -153,7 +154,13 @@ int serve(const EdgeList& data, const std::vector<Update>& stream, const std::ve
     stats.p99_us = pct(0.99) * 1e6;
   }
   stats.device_bytes = used;
-  for (const ServeQueryResult& r : out) stats.queries_admitted += r.admitted ? 1 : 0;
+  for (const ServeQueryResult& r : out) {
+    stats.queries_admitted += r.admitted ? 1 : 0;
+    for (const csm_result& x : r.results) {
+      stats.results++;
+      if (x.status == CSM_ST_CAPPED || x.status == CSM_ST_TIMED_OUT) stats.incomplete++;
+    }
+  }
   // attached queries go before their owner
   for (Ctx& a : att) if (a.h) { csm_gpu_destroy(a.h); a.h = nullptr; }
   return CSM_OK;

@@ -42,6 +42,7 @@ struct ServeConfig {
   uint64_t seed = 7;
   bool want_hash = false;
   bool graphs = true;                    // replay each batch size's launch sequence as a CUDA graph
+  uint64_t deadline_ns = 0;              // per-update search time limit (0: none)
   double max_seconds = 0;                // stop admitting updates after this long (0: run the stream)
 };
 
@@ -57,6 +58,7 @@ struct ServeStats {
   double p50_us = 0, p99_us = 0, mean_batch = 0;
   uint64_t device_bytes = 0;             // owner + admitted queries
   uint32_t queries_admitted = 0, queries_refused = 0;
+  uint64_t results = 0, incomplete = 0;  // (update, query) results, and those CAPPED or TIMED_OUT
 };
 
 // Runs the stream through the serving loop.  Returns CSM_OK or a CSM_E* code
