@@ -264,7 +264,11 @@ def serve_sweep(w, cfg, rates, seconds, *, n_queries, device=0, plugins=None, ca
         if deadline_ms:
             cmd += ["--deadline-ms", str(deadline_ms)]
         t0 = time.perf_counter()
-        p = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=max(180.0, 30 * seconds))
+        except subprocess.TimeoutExpired:
+            out.append({"offered_rate": r, "error": f"serving run exceeded {max(180.0, 30 * seconds):.0f}s"})
+            continue
         if p.returncode != 0:
             out.append({"offered_rate": r, "error": p.stderr[-300:]})
             continue
