@@ -101,6 +101,7 @@ __global__ void k_ix_seed(const uint64_t* __restrict__ keys, uint32_t L, DevGrap
     if (dag->qlab[p] != lx || dag->qlab[ch] != ly) continue;
     atomicOr((unsigned long long*)&b.m1[(uint64_t)ch * b.words + (y >> 6)], 1ull << (y & 63));
     atomicOr((unsigned long long*)&b.m2[(uint64_t)p * b.words + (x >> 6)], 1ull << (x & 63));
+    *b.active = 1u;
   }
 }
 
@@ -109,6 +110,7 @@ __global__ void k_ix_seed(const uint64_t* __restrict__ keys, uint32_t L, DevGrap
 __global__ void k_ix_seed_vertex(uint32_t v, const IxDag* __restrict__ dag, IxBits b) {
   const uint32_t u = threadIdx.x;
   if (u >= dag->nq) return;
+  if (u == 0) *b.active = 1u;
   b.m1[(uint64_t)u * b.words + (v >> 6)] |= 1ull << (v & 63);
   b.m2[(uint64_t)u * b.words + (v >> 6)] |= 1ull << (v & 63);
 }
@@ -117,6 +119,7 @@ __global__ void k_ix_seed_vertex(uint32_t v, const IxDag* __restrict__ dag, IxBi
 // marks its neighbours in S(w, L(u), l(u,p)).  Phase 2 (d2 of u): the same
 // from each child c through d2[c] changes.  One warp per word of changes.
 __global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase) {
+  if (!*b.active) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -148,6 +151,7 @@ __global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
 // whole words of the target bitset, so its updates need no atomics.
 __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase,
                           uint32_t full) {
+  if (!*b.active) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -232,6 +236,15 @@ __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
   }
 }
 
+// End of a round: the change bitsets start the next round empty.
+__global__ void k_ix_clear_changes(IxBits b, uint64_t n) {
+  if (!*b.active) return;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    b.c1[i] = 0;
+    b.c2[i] = 0;
+  }
+}
+
 __global__ void k_ix_popcount(const uint64_t* a, uint64_t n, unsigned long long* out) {
   unsigned long long s = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -291,9 +304,9 @@ static int index_launch_round(IndexState& ix, const DevGraph& g, cudaStream_t st
     k_ix_eval<<<blocks, 256, 0, st>>>(g, ix.d_dag, ix.bits, u, 2, full ? 1u : 0u);
     (*launches)++;
   }
+  k_ix_clear_changes<<<ix.sm_count * 2, 256, 0, st>>>(ix.bits, (uint64_t)nq * ix.words);
+  (*launches)++;
   IXCK(cudaGetLastError());
-  IXCK(cudaMemsetAsync(ix.bits.c1, 0, 8ull * nq * ix.words, st));
-  IXCK(cudaMemsetAsync(ix.bits.c2, 0, 8ull * nq * ix.words, st));
   return CSM_OK;
 }
 
@@ -448,6 +461,9 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   if (rc) return rc;
   rc = mem.alloc((void**)&ix.d_pop, 16);
   if (rc) return rc;
+  rc = mem.alloc((void**)&ix.bits.active, 16);
+  if (rc) return rc;
+  IXCK(cudaMemsetAsync(ix.bits.active, 0xff, 4, st));  // the build evaluates everything
   IXCK(cudaMemsetAsync(ix.bits.d1, 0, 6 * fam, st));
   IXCK(cudaMemcpyAsync(ix.d_dag, &D, sizeof(IxDag), cudaMemcpyHostToDevice, st));
   ix.d2 = ix.bits.d2;
@@ -461,6 +477,7 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
 int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,
                       uint64_t* launches) {
   if (!ix.active || L == 0) return CSM_OK;
+  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
   k_ix_seed<<<(L + 255) / 256, 256, 0, st>>>(keys, L, g, ix.d_dag, ix.bits);
   (*launches)++;
   return index_launch_round(ix, g, st, launches, false);
@@ -469,6 +486,7 @@ int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, u
 int index_vertex_update(IndexState& ix, const DevGraph& g, const csm_update& h, cudaStream_t st, uint64_t* launches) {
   if (!ix.active) return CSM_OK;
   if (h.type != 'v' || h.id1 >= g.n_cap) return CSM_OK;  // a new or a removed vertex: re-evaluate its flags
+  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));
   k_ix_seed_vertex<<<1, 32, 0, st>>>(h.id1, ix.d_dag, ix.bits);
   (*launches)++;
   return index_launch_round(ix, g, st, launches, false);
@@ -499,6 +517,7 @@ void index_free(IndexState& ix, DevMem& mem) {
   if (ix.bits.d1) mem.release(ix.bits.d1, 6 * 8ull * ix.h_dag.nq * ix.words);
   if (ix.d_dag) mem.release(ix.d_dag, sizeof(IxDag));
   if (ix.d_pop) mem.release(ix.d_pop, 16);
+  if (ix.bits.active) mem.release(ix.bits.active, 16);
   ix.bits = IxBits{};
   ix.d_dag = nullptr;
   ix.d_pop = nullptr;

@@ -54,6 +54,7 @@ struct IxDag {
 struct IxBits {
   uint64_t *d1, *d2, *m1, *m2, *c1, *c2;
   uint64_t words;
+  unsigned int* active;  // nonzero when the current round marked anything; else its kernels return at once
 };
 
 struct IndexState {
