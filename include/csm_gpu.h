@@ -90,7 +90,9 @@ typedef struct csm_cfg {
                                  shard_count 0 or 1: no sharding */
   uint32_t donate_every;      /* search hand-over check interval in steps (power of two); 0 = autotuned / 4 */
   uint32_t split_deep;        /* smallest driver range split deep in the search tree; 0 = autotuned / 64 */
-  uint32_t reserved[2];
+  uint32_t enum_capacity;     /* > 0: keep up to this many embeddings of each submit (--print-enum,
+                                 read with csm_gpu_matches); not with CSM_GRAPHS_ON */
+  uint32_t reserved[1];
 } csm_cfg;
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */
@@ -254,6 +256,16 @@ int csm_gpu_index_info(csm_ctx* ctx, csm_index_info* out);
  * ids; out_words must be at least csm_index_info.words.  Waits for the
  * context's stream.  No reference entry point (private members there). */
 int csm_gpu_index_flags(csm_ctx* ctx, uint32_t which, uint64_t* out, uint64_t out_words);
+
+/* Embeddings found by the last submit (the reference's --print-enum output,
+ * ParaCOSM/CSM/matching/SymBi/symbi.cpp:564-569), when cfg.enum_capacity > 0.
+ * Each record is 1 + n_qv uint32 words: the update's index within the last
+ * submit, then the data vertex of each query vertex in query-vertex order.
+ * Copies min(found, enum_capacity, max_records) records to out; *n_found is
+ * every embedding found (more than the capacity means records were dropped).
+ * Order is unspecified; with max_results, an update that reaches the cap may
+ * list more embeddings than its reported count.  Waits for the stream. */
+int csm_gpu_matches(csm_ctx* ctx, uint32_t* out, uint64_t max_records, uint64_t* n_records, uint64_t* n_found);
 
 /* The CUDA stream (cudaStream_t) every launch of this context is issued on,
  * so callers can time work with events on the launching stream. */

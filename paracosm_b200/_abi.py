@@ -66,7 +66,8 @@ class CsmCfg(C.Structure):
         ("shard_count", C.c_uint32),
         ("donate_every", C.c_uint32),
         ("split_deep", C.c_uint32),
-        ("reserved", C.c_uint32 * 2),
+        ("enum_capacity", C.c_uint32),
+        ("reserved", C.c_uint32 * 1),
     ]
 
 
@@ -119,6 +120,8 @@ _SIGNATURES = [
     ("csm_gpu_probe_noalloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("csm_gpu_index_info", C.c_int, [C.c_void_p, C.POINTER(CsmIndexInfo)]),
     ("csm_gpu_index_flags", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]),
+    ("csm_gpu_matches", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint64)]),
     ("csm_gpu_stream", C.c_void_p, [C.c_void_p]),
     ("csm_gpu_search_counters", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     ("csm_gpu_kernel_launches", C.c_uint64, [C.c_void_p]),

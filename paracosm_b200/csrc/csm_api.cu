@@ -138,6 +138,9 @@ struct csm_ctx {
   csm_update* d_gups = nullptr;
   csm_result* d_gres = nullptr;
   csm_update* d_gpad = nullptr;  // padding records: self loops, which are invalid and change nothing
+  // match-set output of the last submit (cfg.enum_capacity > 0)
+  uint32_t* d_enum = nullptr;
+  unsigned long long* d_enum_n = nullptr;
 };
 
 namespace csm {
@@ -268,6 +271,11 @@ static int ensure_batch_buffers(csm_ctx* ctx) {
   AL(ctx->d_gups, sizeof(csm_update) * (size_t)B);
   AL(ctx->d_gres, sizeof(csm_result) * (size_t)B);
   AL(ctx->d_gpad, sizeof(csm_update) * (size_t)B);
+  if (ctx->cfg.enum_capacity) {
+    AL(ctx->d_enum, 4ull * (1 + ctx->nq) * ctx->cfg.enum_capacity);
+    AL(ctx->d_enum_n, 16);
+    CK(cudaMemsetAsync(ctx->d_enum_n, 0, 16, ctx->st));
+  }
   {
     std::vector<csm_update> pad(B, csm_update{'e', 1, 0, 0, 0, 0});
     CK(cudaMemcpyAsync(ctx->d_gpad, pad.data(), sizeof(csm_update) * (size_t)B, cudaMemcpyHostToDevice, ctx->st));
@@ -430,6 +438,11 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   sp.deadline_ns = q->cfg.deadline_ns;
   sp.donate_every = q->cfg.donate_every;
   sp.split_deep = q->cfg.split_deep;
+  if (q->d_enum) {
+    sp.enum_buf = q->d_enum; sp.enum_n = q->d_enum_n; sp.enum_cap = q->cfg.enum_capacity;
+    sp.enum_base = (uint32_t)(out - q->d_results);  // this batch's first update within the submit
+    sp.enum_stride = 1 + q->nq;
+  }
   uint32_t warps, bps;
   search_shape(q, warps, bps);
   if (o->capturing) {  // replays are not timed per search
@@ -683,6 +696,9 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
     if (rc) return rc;
   }
   CK(cudaEventRecord(ctx->ev_start, st));
+  if (ctx->d_enum_n) CK(cudaMemsetAsync(ctx->d_enum_n, 0, 16, st));
+  for (csm_ctx* a : ctx->attached)
+    if (a->d_enum_n) CK(cudaMemsetAsync(a->d_enum_n, 0, 16, st));  // before the fork below
   k_stamp<<<1, 1, 0, st>>>(ctx->d_stamp); CKL();
   for (csm_ctx* a : ctx->attached) {
     rc = stream_after(a->st, st, ctx->ev_fork);
@@ -1081,6 +1097,8 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
   if (cfg->shard_count > 1 && cfg->shard_rank >= cfg->shard_count)
     return set_err(CSM_EINVAL, "shard_rank %u outside shard_count %u", cfg->shard_rank, cfg->shard_count);
+  if (cfg->enum_capacity && cfg->graphs == CSM_GRAPHS_ON)
+    return set_err(CSM_EUNSUPPORTED, "match-set output (enum_capacity) cannot be combined with graph replay");
   if (cfg->turboflux_compat)
     return set_err(CSM_EUNSUPPORTED, "turboflux_compat (the reference TurboFlux deletion count) is not implemented");
   int ndev = 0;
@@ -1211,6 +1229,7 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
   a->cfg.blocks_per_sm = cfg->blocks_per_sm;
   a->cfg.turboflux_compat = cfg->turboflux_compat;
   a->cfg.hbm_budget_bytes = cfg->hbm_budget_bytes;
+  a->cfg.enum_capacity = owner->cfg.graphs == CSM_GRAPHS_ON ? 0u : cfg->enum_capacity;
   a->bmax = owner->bmax;
   a->dev = owner->dev;
   a->sm_count = owner->sm_count;
@@ -1569,6 +1588,22 @@ int csm_gpu_index_flags(csm_ctx* ctx, uint32_t which, uint64_t* out, uint64_t ou
   if (out_words > ix.words)
     for (uint32_t u = 0; u < ix.h_dag.nq; u++)
       memset(out + (uint64_t)u * out_words + ix.words, 0, 8ull * (out_words - ix.words));
+  return CSM_OK;
+}
+
+int csm_gpu_matches(csm_ctx* ctx, uint32_t* out, uint64_t max_records, uint64_t* n_records, uint64_t* n_found) {
+  if (!ctx || !n_records || !n_found || (max_records && !out)) return set_err(CSM_EINVAL, "null argument");
+  if (!ctx->d_enum) return set_err(CSM_ESTATE, "match-set output is off (cfg.enum_capacity = 0)");
+  CK(cudaSetDevice(ctx->dev));
+  int rc = fetch_last(ctx);
+  if (rc) return rc;
+  unsigned long long found = 0;
+  CK(cudaMemcpy(&found, ctx->d_enum_n, 8, cudaMemcpyDeviceToHost));
+  const uint64_t kept = std::min<uint64_t>(found, ctx->cfg.enum_capacity);
+  const uint64_t n = std::min<uint64_t>(kept, max_records);
+  if (n) CK(cudaMemcpy(out, ctx->d_enum, 4ull * (1 + ctx->nq) * n, cudaMemcpyDeviceToHost));
+  *n_records = n;
+  *n_found = found;
   return CSM_OK;
 }
 

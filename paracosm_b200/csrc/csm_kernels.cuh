@@ -131,6 +131,14 @@ struct SearchParams {
   // iterations (a power of two; 0 = 4) and split a driver range deep in the
   // tree only when at least split_deep elements remain (0 = 64)
   uint32_t donate_every, split_deep;
+  // match-set output (null: off): each embedding found at a leaf is appended
+  // as a record of 1 + n_q words (enum_base + its update's batch index, then
+  // the data vertex of every query vertex in query-vertex order) while fewer
+  // than enum_cap records exist; enum_n counts every embedding found
+  uint32_t* enum_buf;
+  unsigned long long* enum_n;
+  unsigned long long enum_cap;
+  uint32_t enum_base, enum_stride;
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,

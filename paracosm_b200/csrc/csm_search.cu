@@ -389,6 +389,20 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     }
     if (pos == n - 1) {
       const uint32_t c = __popc(mask);
+      if (p.enum_buf) {
+        unsigned long long base = 0;
+        if (lane == 0 && c) base = atomicAdd(p.enum_n, (unsigned long long)c);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (valid) {
+          const unsigned long long r = base + __popc(mask & ((1u << lane) - 1u));
+          if (r < p.enum_cap) {
+            uint32_t* rec = p.enum_buf + r * p.enum_stride;
+            rec[0] = p.enum_base + t;
+            rec[1 + A->pos[pos].qv] = x;
+            for (uint32_t q = 0; q < pos; q++) rec[1 + A->pos[q].qv] = m[q];
+          }
+        }
+      }
       if (p.want_hash) {
         unsigned long long h = 0;
         if (valid) {
@@ -450,6 +464,15 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
     if (lane == 0) {
       acc.cnt += 1;
       if (p.want_hash) acc.hash += mix64(pair_hash(A->pos[0].qv, m0) + pair_hash(A->pos[1].qv, m1));
+      if (p.enum_buf) {
+        const unsigned long long r = atomicAdd(p.enum_n, 1ull);
+        if (r < p.enum_cap) {
+          uint32_t* rec = p.enum_buf + r * p.enum_stride;
+          rec[0] = p.enum_base + t;
+          rec[1 + A->pos[0].qv] = m0;
+          rec[1 + A->pos[1].qv] = m1;
+        }
+      }
     }
     return;
   }

@@ -40,7 +40,7 @@ class Engine:
                  deadline_ns: int = 0, hbm_budget_bytes: int = 0, warps_per_block: int = 0,
                  blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0,
                  graphs: bool = False, shard_rank: int = 0, shard_count: int = 1, donate_every: int = 0,
-                 split_deep: int = 0):
+                 split_deep: int = 0, enum_capacity: int = 0):
         self.lib = load_library()
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -62,6 +62,7 @@ class Engine:
         cfg.shard_count = int(shard_count)
         cfg.donate_every = int(donate_every)
         cfg.split_deep = int(split_deep)
+        cfg.enum_capacity = int(enum_capacity)
         self.cfg = cfg
         h = C.c_void_p()
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))
@@ -73,6 +74,7 @@ class Engine:
     # -- setup ---------------------------------------------------------
     def set_query(self, vlabels, edges) -> None:
         vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+        self._nq = len(vl)
         e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
         check(self.lib, self.lib.csm_gpu_set_query(self.h, len(vl), _ptr(vl), len(e), _ptr(e)))
 
@@ -91,7 +93,8 @@ class Engine:
         check(self.lib, self.lib.csm_gpu_build_index(self.h))
 
     def attach(self, vlabels, edges, algorithm: str | int = "parallel_graphflow", *, max_results: int = 0,
-               want_hash: bool = False, warps_per_block: int = 0, blocks_per_sm: int = 0) -> "Engine":
+               want_hash: bool = False, warps_per_block: int = 0, blocks_per_sm: int = 0,
+               enum_capacity: int = 0) -> "Engine":
         """A standing query on this engine's graph; its results follow every submit to this engine."""
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -100,6 +103,7 @@ class Engine:
         cfg.want_hash = int(bool(want_hash))
         cfg.warps_per_block = int(warps_per_block)
         cfg.blocks_per_sm = int(blocks_per_sm)
+        cfg.enum_capacity = int(enum_capacity)
         vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
         e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
         h = C.c_void_p()
@@ -107,6 +111,7 @@ class Engine:
                                                       C.byref(h)))
         a = Engine.__new__(Engine)
         a.lib, a.cfg, a.h, a.submitted, a.attached, a.owner = self.lib, cfg, h, self.submitted, [], self
+        a._nq = len(vl)
         self.attached.append(a)
         return a
 
@@ -207,6 +212,17 @@ class Engine:
             check(self.lib, self.lib.csm_gpu_index_flags(self.h, which, _ptr(buf), words))
             out[key] = np.unpackbits(buf.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)
         return out
+
+    def matches(self, max_records: int | None = None) -> tuple[np.ndarray, int]:
+        """Embeddings of the last submit as rows (update index within the submit, then the data vertex
+        of each query vertex), and the number found (above the capacity when some were dropped)."""
+        if not hasattr(self, "_nq"):
+            raise RuntimeError("set the query first")
+        cap = int(self.cfg.enum_capacity) if max_records is None else int(max_records)
+        n, found = C.c_uint64(), C.c_uint64()
+        buf = np.zeros((max(cap, 1), 1 + self._nq), dtype=np.uint32)
+        check(self.lib, self.lib.csm_gpu_matches(self.h, _ptr(buf), cap, C.byref(n), C.byref(found)))
+        return buf[: int(n.value)], int(found.value)
 
     def stream(self) -> int:
         """cudaStream_t of the engine (for CUDA events on the launching stream)."""

@@ -15,9 +15,11 @@
 // with the shipped BatchUpdates3 (main.cpp:253-397), which skips updates.
 // -t / --auto-tuning pick CPU thread counts in the reference; here -t is
 // accepted and ignored, and --auto-tuning 1 lets the engine choose its
-// launch shape.  --print-enum has no GPU counterpart (the engine counts and
-// hashes embeddings instead of printing them): use --hash 1 and --out.
-// --orders is accepted and ignored (the engine derives its own orders).
+// launch shape.  --print-enum 1 prints every embedding as the reference does
+// ("m0 m1 ... " per line, SymBi/symbi.cpp:564-569), grouped by update, in an
+// unspecified order inside an update; --hash 1 and --out give per-update
+// counts and match-set hashes without printing.  --orders is accepted and
+// ignored (the engine derives its own orders).
 // Files may also be the generator's binary CSMG / CSMU containers.
 #include <sys/resource.h>
 
@@ -108,7 +110,10 @@ int main(int argc, char** argv) {
   }
   (void)thread_num;
   (void)initial_time_limit;
-  if (print_enum) fprintf(stderr, "--print-enum: embeddings are counted and hashed on the GPU, not printed; use --hash 1 --out FILE\n");
+  if (print_enum) {
+    opt.enum_capacity = 1u << 24;  // embeddings kept per chunk of the stream
+    opt.graphs = false;
+  }
 
   auto start = Clock::now();
   printf("----------- Loading graphs ------------\n");
@@ -159,6 +164,7 @@ int main(int argc, char** argv) {
     const size_t b = std::min(stream.size(), a + chunk);
     std::vector<Update> part(stream.begin() + (long)a, stream.begin() + (long)b);
     if (mm->ProcessUpdates(part, res)) break;
+    if (print_enum && mm->PrintMatches(part.size()) != CSM_OK) break;
     for (size_t i = 0; i < part.size(); i++) {
       if (part[i].type == 'v') num_v++; else num_e++;
       if (res[i].pos || res[i].neg) unsafe++;

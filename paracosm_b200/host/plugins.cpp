@@ -1,6 +1,7 @@
 // Plugin classes over the C ABI (see plugins.h).
 #include "plugins.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace csm {
@@ -25,6 +26,8 @@ matching::matching(const EdgeList& query, const EdgeList& data, size_t max_num_r
   cfg.vertex_headroom = opt.vertex_headroom;
   cfg.hbm_budget_bytes = opt.hbm_budget_bytes;
   cfg.deadline_ns = opt.deadline_ns;
+  cfg.enum_capacity = opt.enum_capacity;
+  cfg.graphs = opt.graphs ? CSM_GRAPHS_ON : CSM_GRAPHS_OFF;
   check(csm_gpu_create(&cfg, &ctx_));
 }
 
@@ -120,6 +123,32 @@ int matching::ProcessUpdates(const std::vector<Update>& ups, std::vector<csm_res
   for (const csm_result& r : out) {
     num_positive_results_ += r.pos;
     num_negative_results_ += r.neg;
+  }
+  return CSM_OK;
+}
+
+int matching::PrintMatches(size_t n) {
+  if (err_) return err_;
+  const uint32_t nq = query_.n;
+  uint64_t kept = 0, found = 0;
+  if (check(csm_gpu_matches(ctx_, nullptr, 0, &kept, &found))) return err_;  // sizes first
+  std::vector<uint32_t> rec((size_t)std::min<uint64_t>(found, opt_.enum_capacity) * (1 + nq) + 1);
+  if (check(csm_gpu_matches(ctx_, rec.data(), std::min<uint64_t>(found, opt_.enum_capacity), &kept, &found)))
+    return err_;
+  if (found > kept)
+    fprintf(stderr, "print-enum: %llu embeddings found, %llu kept\n", (unsigned long long)found,
+            (unsigned long long)kept);
+  // group by update (counting sort on the leading word)
+  std::vector<uint64_t> start(n + 1, 0);
+  for (uint64_t r = 0; r < kept; r++) start[rec[r * (1 + nq)] + 1]++;
+  for (size_t i = 0; i < n; i++) start[i + 1] += start[i];
+  std::vector<uint64_t> order(kept), fill(start.begin(), start.end() - 1);
+  for (uint64_t r = 0; r < kept; r++) order[fill[rec[r * (1 + nq)]]++] = r;
+  std::string line;
+  for (uint64_t r : order) {
+    line.clear();
+    for (uint32_t q = 0; q < nq; q++) { line += std::to_string(rec[r * (1 + nq) + 1 + q]); line += ' '; }
+    puts(line.c_str());
   }
   return CSM_OK;
 }

@@ -37,6 +37,8 @@ struct GpuOptions {
   uint32_t vertex_headroom = 0;
   uint64_t hbm_budget_bytes = 0;
   uint64_t deadline_ns = 0;
+  uint32_t enum_capacity = 0;  // > 0: keep embeddings for PrintMatches (the reference's --print-enum)
+  bool graphs = false;         // replay each batch size's launch sequence as a CUDA graph
 };
 
 class matching {
@@ -64,6 +66,9 @@ class matching {
 
   // Runs `ups` in order as batches; out[i] is the result of ups[i].
   int ProcessUpdates(const std::vector<Update>& ups, std::vector<csm_result>& out);
+  // Prints the embeddings of the last ProcessUpdates of n updates, update by
+  // update, one "m0 m1 ... " line each (needs GpuOptions::enum_capacity).
+  int PrintMatches(size_t n);
 
   int error() const { return err_; }
   const std::string& error_text() const { return err_text_; }

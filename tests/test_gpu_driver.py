@@ -39,3 +39,16 @@ def test_driver_output_matches_the_reference(tmp_path, algo, mode):
     assert np.array_equal(np.array([int(r_["hash"]) for r_ in rows], dtype=np.uint64), x["symbi_hash"])
     if algo != "parallel_graphflow":
         assert "DAG: " in lines
+
+
+def test_driver_print_enum_lists_every_embedding():
+    g = load_golden("dense_del")
+    r = subprocess.run([str(CSM), "-q", "query.graph", "-d", "data.graph", "-u", "stream.txt", "-a", "parallel_symbi",
+                        "--print-enum", "1", "--report-initial", "0", "--print-prep", "0"],
+                       cwd=g["dir"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    nq = len(g["qv"])
+    rows = [ln.split() for ln in r.stdout.splitlines() if ln.strip() and all(t.isdigit() for t in ln.split())]
+    rows = [x for x in rows if len(x) == nq]
+    x = g["exp"]
+    assert len(rows) == int((x["symbi_pos"] + x["symbi_neg"]).sum())

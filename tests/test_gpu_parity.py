@@ -217,3 +217,38 @@ def test_turboflux_compat_is_refused():
     with pytest.raises(CsmError) as e:
         Engine("parallel_turboflux", turboflux_compat=True)
     assert e.value.code == CSM_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("case", ["c1_small", "mixed_2el", "dense_del", "zipf_8q"])
+def test_match_sets_rebuild_the_reference_hash(case, algo):
+    """The embeddings the engine emits (the reference's --print-enum output) are, per update,
+    exactly the counted ones: their number is the update's count and their canonical hash is
+    sequential SymBi's (golden)."""
+    g = load_golden(case)
+    x = g["exp"]
+    with Engine(algo, enum_capacity=1 << 20, max_batch=97) as eng:
+        eng.set_query(g["qv"], g["qe"])
+        eng.load_graph(g["vl"], g["e"])
+        eng.build_index()
+        res = eng.run(g["stream"])
+        rec, found = eng.matches()
+    total = int((x["symbi_pos"] + x["symbi_neg"]).sum())
+    assert found == total == len(rec)
+    assert np.array_equal(res["pos"], x["symbi_pos"]) and np.array_equal(res["neg"], x["symbi_neg"])
+    n_q = len(g["qv"])
+    per = np.bincount(rec[:, 0], minlength=len(g["stream"]))
+    assert np.array_equal(per, (x["symbi_pos"] + x["symbi_neg"]).astype(np.int64))
+    # the canonical per-update hash, recomputed on the host from the emitted embeddings
+    def mix64(z):
+        z = z ^ (z >> np.uint64(33)); z = z * np.uint64(0xff51afd7ed558ccd)
+        z = z ^ (z >> np.uint64(33)); z = z * np.uint64(0xc4ceb9fe1a85ec53)
+        return z ^ (z >> np.uint64(33))
+    with np.errstate(over="ignore"):
+        s = np.zeros(len(rec), dtype=np.uint64)
+        for q in range(n_q):
+            s += mix64((np.uint64(q + 1) << np.uint64(32)) ^ rec[:, 1 + q].astype(np.uint64) ^
+                       np.uint64(0x9E3779B97F4A7C15))
+        h = np.zeros(len(g["stream"]), dtype=np.uint64)
+        np.add.at(h, rec[:, 0], mix64(s))
+    assert np.array_equal(h, x["symbi_hash"]), np.nonzero(h != x["symbi_hash"])[0][:10]
