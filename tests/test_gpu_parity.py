@@ -227,7 +227,7 @@ def test_match_sets_rebuild_the_reference_hash(case, algo):
     sequential SymBi's (golden)."""
     g = load_golden(case)
     x = g["exp"]
-    with Engine(algo, enum_capacity=1 << 20, max_batch=97) as eng:
+    with Engine(algo, enum_capacity=1 << 22, max_batch=97) as eng:
         eng.set_query(g["qv"], g["qe"])
         eng.load_graph(g["vl"], g["e"])
         eng.build_index()
