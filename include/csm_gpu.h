@@ -75,10 +75,11 @@ typedef struct csm_cfg {
   uint32_t max_batch;         /* updates per batch in CSM_MODE_BATCHED (<= 65536); 0 = 65536 */
   int32_t want_hash;          /* != 0: compute the per-update match-set hash */
   int32_t device;             /* CUDA device ordinal */
-  int32_t turboflux_compat;   /* reserved: would reproduce the reference TurboFlux deletion
-                                 count, which ignores the anchor edge label
-                                 (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:975);
-                                 != 0 is refused with CSM_EUNSUPPORTED */
+  int32_t turboflux_compat;   /* != 0: reproduce the reference TurboFlux deletion count, which
+                                 seeds every query edge whose vertex labels match, ignoring the
+                                 anchor's edge label, and filters anchor endpoints by d2 only on
+                                 spanning-tree edges (ParaCOSM/CSM/matching/TurboFlux/
+                                 turboflux.cpp:966-1022); TurboFlux in CSM_MODE_PLAIN only */
   uint32_t warps_per_block;   /* search kernel tuning; 0 = autotuned */
   uint32_t blocks_per_sm;     /* search kernel tuning; 0 = autotuned */
   uint32_t vertex_headroom;   /* vertex slots beyond the loaded graph for 'v' updates; 0 = 1024 */

@@ -422,7 +422,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   if (rc) return rc;
   k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, o->d_info, g, q->d_plan, q->index.d2, q->index.words,
                                               q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error,
-                                              q->cfg.shard_rank, q->cfg.shard_count); CKL();
+                                              q->cfg.shard_rank, q->cfg.shard_count,
+                                              (uint32_t)q->cfg.turboflux_compat); CKL();
   SearchParams sp{};
   sp.g = g; sp.plan = q->d_plan; sp.tasks = q->d_tasks; sp.n_tasks = c + 6; sp.task_cap = q->task_cap;
   sp.task_next = c + 7; sp.info = o->d_info; sp.count = q->d_count; sp.hash = q->d_hash; sp.bytes = q->d_bytes;
@@ -1099,8 +1100,9 @@ int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
     return set_err(CSM_EINVAL, "shard_rank %u outside shard_count %u", cfg->shard_rank, cfg->shard_count);
   if (cfg->enum_capacity && cfg->graphs == CSM_GRAPHS_ON)
     return set_err(CSM_EUNSUPPORTED, "match-set output (enum_capacity) cannot be combined with graph replay");
-  if (cfg->turboflux_compat)
-    return set_err(CSM_EUNSUPPORTED, "turboflux_compat (the reference TurboFlux deletion count) is not implemented");
+  if (cfg->turboflux_compat && (cfg->algorithm != CSM_ALGO_TURBOFLUX || cfg->mode != CSM_MODE_PLAIN))
+    return set_err(CSM_EUNSUPPORTED, "turboflux_compat needs the TurboFlux plugin in CSM_MODE_PLAIN (its deletion "
+                                     "count depends on the exact index at each update)");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(CSM_ECUDA, "no CUDA device");
   if (cfg->device < 0 || cfg->device >= ndev) return set_err(CSM_EINVAL, "bad device %d", cfg->device);
@@ -1403,7 +1405,21 @@ int csm_gpu_build_index(csm_ctx* ctx) {
   for (uint32_t u = 0; u < ctx->nq; u++)
     for (uint32_t l : ctx->qel[u]) qel_f[u].push_back(fold_host(ctx->qlab_e, l));
   IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &qel_f};
-  return index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->sm_count, ctx->st, &ctx->launches);
+  rc = index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->sm_count, ctx->st, &ctx->launches);
+  if (rc || !ctx->cfg.turboflux_compat) return rc;
+  // compat deletions need to know which anchors are spanning-tree edges
+  const IxDag& D = ctx->index.h_dag;
+  for (uint32_t a = 0; a < ctx->h_plan->n_anchor; a++) {
+    PlanAnchor& A = ctx->h_plan->anchors[a];
+    const uint32_t x = A.pos[0].qv, y = A.pos[1].qv;
+    bool tree = false;
+    for (uint32_t k = 0; k < D.npar[y]; k++) tree |= D.par[y][k] == x;
+    for (uint32_t k = 0; k < D.npar[x]; k++) tree |= D.par[x][k] == y;
+    A.tree = tree ? 1u : 0u;
+  }
+  CK(cudaMemcpyAsync(ctx->d_plan, ctx->h_plan, ctx->plan_bytes, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return CSM_OK;
 }
 
 int csm_gpu_initial_match(csm_ctx* ctx, uint64_t* count) {

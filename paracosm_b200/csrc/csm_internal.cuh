@@ -197,6 +197,7 @@ struct PlanPos {
 
 struct PlanAnchor {
   uint32_t la, lb, el;       // label triple of the anchor (pos 0 label, pos 1 label, edge label)
+  uint32_t tree;             // the anchor is an edge of the TurboFlux spanning tree (compat deletions)
   PlanPos pos[kMaxQ];
   uint8_t back_pos[kMaxQE];
   uint16_t back_combo[kMaxQE];

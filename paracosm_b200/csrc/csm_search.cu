@@ -45,7 +45,8 @@ __device__ __forceinline__ bool d2_bit(const uint64_t* d2, uint64_t words, uint3
 
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
-                       uint32_t* safe, unsigned int* error, uint32_t shard_rank, uint32_t shard_count) {
+                       uint32_t* safe, unsigned int* error, uint32_t shard_rank, uint32_t shard_count,
+                       uint32_t turboflux_compat) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
@@ -53,9 +54,13 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
   if ((u.flags & UF_VALID) && !(u.flags & UF_INVALID)) {
     const uint32_t L1 = g.vlabel[u.v1], L2 = g.vlabel[u.v2], l = u.label;
     const uint32_t na = plan->n_anchor;
+    // The reference's TurboFlux deletion seeds every query edge whose vertex
+    // labels match, whatever its edge label, and filters the endpoints by d2
+    // only on spanning-tree edges (ParaCOSM/CSM/matching/TurboFlux/turboflux.cpp:966-1022)
+    const bool compat_del = turboflux_compat && !(u.flags & UF_ADD);
     for (uint32_t a = 0; a < na; a++) {
       const PlanAnchor* A = &plan->anchors[a];
-      if (A->el != l) continue;
+      if (A->el != l && !compat_del) continue;
       const bool o0 = A->la == L1 && A->lb == L2;
       const bool o1 = A->la == L2 && A->lb == L1;
       if (!(o0 || o1)) continue;
@@ -63,7 +68,9 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
       for (int o = 0; o < 2; o++) {
         if (!(o ? o1 : o0)) continue;
         const uint32_t x = o ? u.v2 : u.v1, y = o ? u.v1 : u.v2;
-        if (d2 && !(d2_bit(d2, d2_words, A->pos[0].qv, x) && d2_bit(d2, d2_words, A->pos[1].qv, y))) continue;
+        if (d2 && (!compat_del || A->tree) &&
+            !(d2_bit(d2, d2_words, A->pos[0].qv, x) && d2_bit(d2, d2_words, A->pos[1].qv, y)))
+          continue;
         if (shard_count > 1 && (s + 2 * a + (uint32_t)o) % shard_count != shard_rank) continue;  // another GPU's
         unsigned int i = atomicAdd(n_tasks, 1u);
         if (i >= task_cap) { atomicExch(error, kErrTaskOverflow); continue; }

@@ -212,11 +212,12 @@ def test_deadline_reports_timed_out_with_lower_bounds():
     assert_same(res2, ref["pos"], ref["neg"], ref["hash"])
 
 
-def test_turboflux_compat_is_refused():
+def test_turboflux_compat_needs_the_plain_turboflux_form():
     from paracosm_b200._abi import CSM_EUNSUPPORTED, CsmError
-    with pytest.raises(CsmError) as e:
-        Engine("parallel_turboflux", turboflux_compat=True)
-    assert e.value.code == CSM_EUNSUPPORTED
+    for kw in ({"algorithm": "parallel_turboflux"}, {"algorithm": "parallel_symbi", "mode": "plain"}):
+        with pytest.raises(CsmError) as e:
+            Engine(turboflux_compat=True, **kw)
+        assert e.value.code == CSM_EUNSUPPORTED
 
 
 @pytest.mark.parametrize("algo", ALGOS)
@@ -252,3 +253,15 @@ def test_match_sets_rebuild_the_reference_hash(case, algo):
         h = np.zeros(len(g["stream"]), dtype=np.uint64)
         np.add.at(h, rec[:, 0], mix64(s))
     assert np.array_equal(h, x["symbi_hash"]), np.nonzero(h != x["symbi_hash"])[0][:10]
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_turboflux_compat_reproduces_the_reference_turboflux(case):
+    """With turboflux_compat (one update per launch), positives, negatives and hashes equal the
+    reference's sequential TurboFlux, whose deletions ignore the anchor edge's label."""
+    g = load_golden(case)
+    cap = g["params"]["max_results"] or 0
+    res, _ = run_engine(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], "parallel_turboflux", mode="plain",
+                        max_results=cap, homo=g["params"]["homo"], turboflux_compat=True)
+    x = g["exp"]
+    assert_same(res, x["turboflux_pos"], x["turboflux_neg"], x["turboflux_hash"], cap)
