@@ -272,6 +272,10 @@ int csm_gpu_matches(csm_ctx* ctx, uint32_t* out, uint64_t max_records, uint64_t*
  * so callers can time work with events on the launching stream. */
 void* csm_gpu_stream(csm_ctx* ctx);
 
+/* *done = 1 when every submitted update has a result (the submit's work on
+ * the device has finished), else 0; does not block. */
+int csm_gpu_poll(csm_ctx* ctx, int* done);
+
 /* Waits until every submitted update has a result, or timeout_ns passes
  * (0 = no limit). */
 int csm_gpu_wait(csm_ctx* ctx, uint64_t timeout_ns);

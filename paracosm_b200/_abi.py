@@ -113,6 +113,7 @@ _SIGNATURES = [
     ("csm_gpu_classify", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("csm_gpu_submit", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
     ("csm_gpu_submit_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("csm_gpu_poll", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("csm_gpu_wait", C.c_int, [C.c_void_p, C.c_uint64]),
     ("csm_gpu_results", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p]),
     ("csm_gpu_results_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),

@@ -1490,6 +1490,17 @@ int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups) {
   return submit_common(ctx, n, d_ups, nullptr);
 }
 
+int csm_gpu_poll(csm_ctx* ctx, int* done) {
+  if (!ctx || !done) return set_err(CSM_EINVAL, "null argument");
+  CK(cudaSetDevice(ctx->dev));
+  cudaError_t e = cudaEventQuery(ctx->ev_end);
+  if (e == cudaSuccess && ctx->owner) e = cudaEventQuery(ctx->owner->ev_end);  // the owner issues its work
+  if (e == cudaErrorNotReady) { *done = 0; return CSM_OK; }
+  if (e != cudaSuccess) return set_err(CSM_ECUDA, "poll: %s", cudaGetErrorString(e));
+  *done = 1;
+  return CSM_OK;
+}
+
 int csm_gpu_wait(csm_ctx* ctx, uint64_t timeout_ns) {
   if (!ctx) return set_err(CSM_EINVAL, "null context");
   if (timeout_ns) {

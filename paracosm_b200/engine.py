@@ -164,6 +164,12 @@ class Engine:
         for a in self.attached:
             a.submitted += n
 
+    def poll(self) -> bool:
+        """True when every submitted update has a result (does not block)."""
+        d = C.c_int()
+        check(self.lib, self.lib.csm_gpu_poll(self.h, C.byref(d)))
+        return bool(d.value)
+
     def wait(self, timeout_ns: int = 0) -> None:
         check(self.lib, self.lib.csm_gpu_wait(self.h, timeout_ns))
 

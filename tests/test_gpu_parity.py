@@ -265,3 +265,20 @@ def test_turboflux_compat_reproduces_the_reference_turboflux(case):
                         max_results=cap, homo=g["params"]["homo"], turboflux_compat=True)
     x = g["exp"]
     assert_same(res, x["turboflux_pos"], x["turboflux_neg"], x["turboflux_hash"], cap)
+
+
+def test_poll_reports_completion_without_blocking():
+    import time
+    g = load_golden("zipf_8q")
+    with Engine("parallel_symbi", want_hash=True) as eng:
+        eng.set_query(g["qv"], g["qe"])
+        eng.load_graph(g["vl"], g["e"])
+        eng.build_index()
+        first = eng.submit(g["stream"])
+        t0 = time.time()
+        while not eng.poll():
+            assert time.time() - t0 < 60
+            time.sleep(0.001)
+        res = eng.results(first, len(g["stream"]))
+    x = g["exp"]
+    assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"])
