@@ -403,7 +403,7 @@ static void search_shape(const csm_ctx* q, uint32_t& warps, uint32_t& bps) {
   warps = q->cfg.warps_per_block ? q->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   bps = q->cfg.blocks_per_sm ? q->cfg.blocks_per_sm : 0;
-  if (!bps) bps = std::max<uint32_t>(1, search_max_blocks(q->nq, warps));
+  if (!bps) bps = std::max<uint32_t>(1, search_max_blocks(q->nq, warps, q->d_enum != nullptr));
 }
 
 // One standing query q over the owner o's union graph: index to the union

@@ -288,7 +288,10 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
 }
 
 // Depth-first walk over chunked levels starting at level `d` (see the file
-// comment); positions 0 and 1 hold m0 and m1.
+// comment); positions 0 and 1 hold m0 and m1.  EN compiles the match-set
+// append in: it is a separate instantiation so that the counting-only kernel
+// keeps its register budget.
+template <bool EN>
 __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int d, uint32_t lane,
                            const Task& T, const PlanAnchor* A, uint32_t m0, uint32_t m1, TaskAcc& acc) {
   const uint32_t n = p.plan->n;
@@ -396,7 +399,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     }
     if (pos == n - 1) {
       const uint32_t c = __popc(mask);
-      if (p.enum_buf) {
+      if (EN) {
         unsigned long long base = 0;
         if (lane == 0 && c) base = atomicAdd(p.enum_n, (unsigned long long)c);
         base = __shfl_sync(0xffffffffu, base, 0);
@@ -460,6 +463,7 @@ __device__ __forceinline__ void flush_acc(const SearchParams& p, uint32_t t, uin
 
 // Root task: positions 0 and 1 are the updated edge; level 1 holds the driver
 // segment of position 2.
+template <bool EN>
 __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, const Task& T,
                          TaskAcc& acc) {
   const uint32_t n = p.plan->n;
@@ -471,7 +475,7 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
     if (lane == 0) {
       acc.cnt += 1;
       if (p.want_hash) acc.hash += mix64(pair_hash(A->pos[0].qv, m0) + pair_hash(A->pos[1].qv, m1));
-      if (p.enum_buf) {
+      if (EN) {
         const unsigned long long r = atomicAdd(p.enum_n, 1ull);
         if (r < p.enum_cap) {
           uint32_t* rec = p.enum_buf + r * p.enum_stride;
@@ -513,12 +517,13 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
     lv[1].dlo[0] = dlo0; lv[1].dn[0] = minsz; lv[1].dsel[0] = (uint8_t)sel;
   }
   __syncwarp();
-  run_levels(p, pool, lv, 1, lane, T, A, m0, m1, acc);
+  run_levels<EN>(p, pool, lv, 1, lane, T, A, m0, m1, acc);
 }
 
 // Donated task: rebuild the chain of the partial match (exhausted levels
 // 1 .. depth-1) and continue from level `depth`.  `hw` holds record words
 // 0..4 in lanes 0..4 and `mv` holds m[lane] (see DTask).
+template <bool EN>
 __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, uint32_t hw,
                             uint32_t mv, TaskAcc& acc, uint32_t& upd_out, unsigned long long ticket,
                             unsigned long long seen_seq) {
@@ -560,7 +565,7 @@ __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM
   const unsigned int stopped =
       __shfl_sync(0xffffffffu, lane == 0 ? *(volatile unsigned int*)(p.stop + upd) : 0u, 0);
   if (stopped) return;
-  run_levels(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
+  run_levels<EN>(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
 }
 
 // Per launch: tickets keep counting up across launches (the ring's slot
@@ -573,7 +578,7 @@ __global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint3
   ss->launch_t0 = global_ns();
 }
 
-template <int W>
+template <int W, bool EN>
 __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint4 task_scratch[W * 10];  // one 160-byte record per warp
@@ -600,7 +605,7 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
       atomicCAS(const_cast<unsigned int*>(stop) + T.upd, 0u, kStopDeadline);
     // stop flags change under our feet: one lane reads, the warp follows it
     const unsigned int stopped = __shfl_sync(0xffffffffu, lane == 0 ? stop[T.upd] : 0u, 0);
-    if (!stopped) run_root(p, pool, lv, lane, T, acc);
+    if (!stopped) run_root<EN>(p, pool, lv, lane, T, acc);
     const unsigned long long te = global_ns();
     busy_ns += te - tb;
     root_ns += te - tb;
@@ -671,7 +676,7 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
     __syncwarp();
     uint32_t t = 0;
     const unsigned long long tb = global_ns();
-    run_donated(p, pool, lv, lane, hw, mv, acc, t, claimed, seen);
+    run_donated<EN>(p, pool, lv, lane, hw, mv, acc, t, claimed, seen);
     busy_ns += global_ns() - tb;
     max_task = max(max_task, global_ns() - tb);
     if (t < p.batch) flush_acc(p, t, lane, acc);
@@ -689,23 +694,33 @@ __global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
 
 // Blocks of the search kernel that can be resident on one SM for this query
 // size (registers, shared memory and warp slots), from the occupancy API.
-uint32_t search_max_blocks(uint32_t n_q, uint32_t warps) {
+namespace {
+
+template <int W, bool EN>
+cudaError_t search_occupancy(int* nb, size_t smem) {
+  cudaFuncSetAttribute(k_search<W, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_search<W, EN>, W * 32, smem);
+}
+
+template <int W, bool EN>
+void search_launch(const SearchParams& p, uint32_t blocks, size_t smem, cudaStream_t s) {
+  cudaFuncSetAttribute(k_search<W, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_search<W, EN><<<blocks, W * 32, smem, s>>>(p);
+}
+
+}  // namespace
+
+// Blocks of the search kernel that can be resident on one SM for this query
+// size (registers, shared memory and warp slots), from the occupancy API.
+// `with_enum` selects the instantiation that appends match sets.
+uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, bool with_enum) {
   const size_t smem = search_smem_bytes(n_q, warps);
   int nb = 0;
   cudaError_t e = cudaSuccess;
   switch (warps) {
-    case 4:
-      cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<4>, 4 * 32, smem);
-      break;
-    case 16:
-      cudaFuncSetAttribute(k_search<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<16>, 16 * 32, smem);
-      break;
-    default:
-      cudaFuncSetAttribute(k_search<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<8>, 8 * 32, smem);
-      break;
+    case 4: e = with_enum ? search_occupancy<4, true>(&nb, smem) : search_occupancy<4, false>(&nb, smem); break;
+    case 16: e = with_enum ? search_occupancy<16, true>(&nb, smem) : search_occupancy<16, false>(&nb, smem); break;
+    default: e = with_enum ? search_occupancy<8, true>(&nb, smem) : search_occupancy<8, false>(&nb, smem); break;
   }
   if (e != cudaSuccess) { cudaGetLastError(); return 0; }
   return (uint32_t)nb;
@@ -714,19 +729,11 @@ uint32_t search_max_blocks(uint32_t n_q, uint32_t warps) {
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s) {
   const size_t smem = search_smem_bytes(n_q, warps);
   if (p.q) k_search_prep<<<1, 1, 0, s>>>(p.q, p.n_tasks, p.task_cap, p.sstat, p.error);
+  const bool en = p.enum_buf != nullptr;
   switch (warps) {
-    case 4:
-      cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_search<4><<<blocks, 4 * 32, smem, s>>>(p);
-      break;
-    case 16:
-      cudaFuncSetAttribute(k_search<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_search<16><<<blocks, 16 * 32, smem, s>>>(p);
-      break;
-    default:
-      cudaFuncSetAttribute(k_search<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_search<8><<<blocks, 8 * 32, smem, s>>>(p);
-      break;
+    case 4: en ? search_launch<4, true>(p, blocks, smem, s) : search_launch<4, false>(p, blocks, smem, s); break;
+    case 16: en ? search_launch<16, true>(p, blocks, smem, s) : search_launch<16, false>(p, blocks, smem, s); break;
+    default: en ? search_launch<8, true>(p, blocks, smem, s) : search_launch<8, false>(p, blocks, smem, s); break;
   }
 }
 
