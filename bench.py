@@ -314,7 +314,9 @@ def run_stress_config(args, cfg):
     from paracosm_b200 import ST_CAPPED, ST_TIMED_OUT, Engine
     B, W, K = cfg["batch"], args.warmup, args.steps
     w = get_workload(cfg, max(cfg["min_updates"], (W + K) * B))
-    plugins = ["parallel_symbi", "parallel_turboflux", "parallel_graphflow"]
+    # the CaLiG-style plugin on two of the four queries (C5 names the CaLiG- and
+    # NewSP-style plugins; there is no NewSP-style plugin here)
+    plugins = ["parallel_calig", "parallel_turboflux", "parallel_symbi", "parallel_calig"]
     t0 = time.perf_counter()
     own = Engine(plugins[0], max_results=cfg["max_results"], max_batch=B, deadline_ns=cfg["deadline_ns"],
                  graphs=True)
@@ -325,7 +327,8 @@ def run_stress_config(args, cfg):
     own.reserve_labels(np.unique(vls), np.unique(els))
     own.load_graph(w.vlabels, w.edges)
     own.build_index()
-    att = [own.attach(*w.queries[i], plugins[i % 3], max_results=cfg["max_results"]) for i in range(1, len(w.queries))]
+    att = [own.attach(*w.queries[i], plugins[i % len(plugins)], max_results=cfg["max_results"])
+           for i in range(1, len(w.queries))]
     log(f"engine with {len(w.queries)} queries ready in {time.perf_counter() - t0:.1f}s")
     for i in range(W):
         own.run(w.stream[i * B:(i + 1) * B])
@@ -344,7 +347,7 @@ def run_stress_config(args, cfg):
         r = np.concatenate(rs)
         bad = (r["status"] == ST_CAPPED) | (r["status"] == ST_TIMED_OUT)
         per_q.append({"query": i, "vertices": int(len(w.queries[i][0])), "edges": int(len(w.queries[i][1])),
-                      "plugin": plugins[i % 3], "success_rate": float(1 - bad.mean()),
+                      "plugin": plugins[i % len(plugins)], "success_rate": float(1 - bad.mean()),
                       "capped": int((r["status"] == ST_CAPPED).sum()),
                       "timed_out": int((r["status"] == ST_TIMED_OUT).sum()),
                       "p50_us": float(np.percentile(r["latency_ns"], 50)) / 1e3,

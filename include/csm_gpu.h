@@ -58,6 +58,8 @@ extern "C" {
 #define CSM_ALGO_GRAPHFLOW 0 /* -a parallel_graphflow / graphflow: no index */
 #define CSM_ALGO_TURBOFLUX 1 /* -a parallel_turboflux / turboflux: DCG over a query spanning tree */
 #define CSM_ALGO_SYMBI 2     /* -a parallel_symbi / symbi: DCS over a DAG of all query edges */
+#define CSM_ALGO_CALIG 3     /* -a parallel_calig / calig: CaLiG-style lighting filter over every query edge;
+                                an insertion of a present edge counts 0 (Parallel_CaLiG/parallel_calig.cpp:1233) */
 
 /* ---- execution modes ------------------------------------------------ */
 #define CSM_MODE_BATCHED 0   /* many updates per launch sequence (default) */

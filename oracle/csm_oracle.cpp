@@ -3,6 +3,8 @@
 #include "csm_oracle.h"
 
 #include <algorithm>
+#include <functional>
+#include <map>
 #include <cstring>
 #include <vector>
 
@@ -609,6 +611,155 @@ extern "C" int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n
       if (d1[u][v]) d1_out[u * words + (v >> 6)] |= 1ULL << (v & 63);
       if (d2[u][v]) d2_out[u * words + (v >> 6)] |= 1ULL << (v & 63);
     }
+  }
+  return (int)n;
+}
+
+namespace {
+
+// Can the query neighbours of u be mapped to distinct neighbours w of v, each
+// over an edge with the query edge's label, onto a vertex with the query
+// neighbour's label and lit[uj][w]?  (Without injectivity under homo.)
+// Augmenting paths over the query side (at most 31 neighbours).
+bool calig_inject(const QueryGraph& q, const Graph& g, uint32_t u, uint32_t v,
+                  const std::vector<std::vector<char>>& lit, bool homo) {
+  const auto& qn = q.nbr[u];
+  const auto& ql = q.elab[u];
+  const auto& dn = g.nbr[v];
+  const auto& dl = g.elab[v];
+  auto fits = [&](size_t i, size_t j) {
+    const uint32_t uj = qn[i], w = dn[j];
+    return dl[j] == ql[i] && g.label(w) == q.vlabel[uj] && lit[uj][w];
+  };
+  if (homo) {
+    for (size_t i = 0; i < qn.size(); i++) {
+      bool any = false;
+      for (size_t j = 0; j < dn.size() && !any; j++) any = fits(i, j);
+      if (!any) return false;
+    }
+    return true;
+  }
+  if (qn.size() > dn.size()) return false;
+  std::vector<int> owner(dn.size(), -1);  // data neighbour -> query neighbour index
+  for (size_t i = 0; i < qn.size(); i++) {
+    std::vector<char> seen(dn.size(), 0);
+    std::function<bool(size_t)> augment = [&](size_t a) {
+      for (size_t j = 0; j < dn.size(); j++) {
+        if (seen[j] || !fits(a, j)) continue;
+        seen[j] = 1;
+        if (owner[j] < 0 || augment((size_t)owner[j])) { owner[j] = (int)a; return true; }
+      }
+      return false;
+    };
+    if (!augment(i)) return false;
+  }
+  return true;
+}
+
+// The lighting of CaLiG after static filtering (constructCand + staticFilter,
+// ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:337-361, 385-396,
+// 398-429, 970-975): the greatest set of (u, v) pairs with L(v) = L(u) such
+// that every lit (u, v) can map u's query neighbours to distinct lit
+// neighbours of v.  The reference checks one candidate per neighbour
+// (checkNei) plus distinct witnesses inside each group of same-label
+// neighbours (tryNei over rep_nei); witnesses of different labels are
+// distinct anyway, so that is one injective map of the whole neighbourhood.
+void calig_fixpoint(const QueryGraph& q, const Graph& g, bool homo, std::vector<std::vector<char>>& lit) {
+  const size_t n = g.vlabel.size();
+  lit.assign(q.n, std::vector<char>(n, 0));
+  for (uint32_t u = 0; u < q.n; u++)
+    for (size_t v = 0; v < n; v++) lit[u][v] = g.vlabel[v] != NOT_EXIST && g.vlabel[v] == q.vlabel[u];
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (uint32_t u = 0; u < q.n; u++)
+      for (uint32_t v = 0; v < n; v++)
+        if (lit[u][v] && !calig_inject(q, g, u, v, lit, homo)) { lit[u][v] = 0; changed = true; }
+  }
+}
+
+// The two bounded levels the engine maintains for its CaLiG-style plugin
+// (a sound superset of the lighting above, exact under every update):
+//   li0[u][v]: L(v) = L(u) and, for every (vertex label, edge label) pair c
+//              of u's query edges, v has at least as many neighbours of
+//              pair c as u has (one under homo);
+//   li1[u][v]: li0[u][v] and every query neighbour uj of u has a neighbour w
+//              of v over an edge labelled l(u, uj) with li0[uj][w].
+void calig_levels(const QueryGraph& q, const Graph& g, bool homo, std::vector<std::vector<char>>& li0,
+                  std::vector<std::vector<char>>& li1) {
+  const size_t n = g.vlabel.size();
+  li0.assign(q.n, std::vector<char>(n, 0));
+  li1.assign(q.n, std::vector<char>(n, 0));
+  for (uint32_t u = 0; u < q.n; u++) {
+    std::map<std::pair<uint32_t, uint32_t>, uint32_t> need;
+    for (size_t i = 0; i < q.nbr[u].size(); i++) need[{q.vlabel[q.nbr[u][i]], q.elab[u][i]}]++;
+    for (size_t v = 0; v < n; v++) {
+      if (g.vlabel[v] == NOT_EXIST || g.vlabel[v] != q.vlabel[u]) continue;
+      bool ok = true;
+      for (const auto& kv : need) {
+        uint32_t have = 0;
+        for (size_t j = 0; j < g.nbr[v].size(); j++)
+          if (g.elab[v][j] == kv.first.second && g.label(g.nbr[v][j]) == kv.first.first) have++;
+        if (have < (homo ? 1u : kv.second)) { ok = false; break; }
+      }
+      li0[u][v] = ok;
+    }
+  }
+  for (uint32_t u = 0; u < q.n; u++)
+    for (uint32_t v = 0; v < n; v++) {
+      if (!li0[u][v]) continue;
+      bool ok = true;
+      for (size_t i = 0; i < q.nbr[u].size() && ok; i++)
+        ok = has_support(g, v, q.vlabel[q.nbr[u][i]], q.elab[u][i], li0[q.nbr[u][i]]);
+      li1[u][v] = ok;
+    }
+}
+
+void pack_bits(const std::vector<std::vector<char>>& f, uint64_t words, uint64_t* out) {
+  for (size_t u = 0; u < f.size(); u++) {
+    for (uint64_t w = 0; w < words; w++) out[u * words + w] = 0;
+    for (size_t v = 0; v < f[u].size(); v++)
+      if (f[u][v]) out[u * words + (v >> 6)] |= 1ULL << (v & 63);
+  }
+}
+
+}  // namespace
+
+extern "C" int oracle_calig_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                                  uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                                  uint64_t n_up, const oracle_update* ups, int homo, uint64_t words, uint64_t* li0_out,
+                                  uint64_t* li1_out, uint64_t* lit_out) {
+  QueryGraph q;
+  if (n_qv < 2 || n_qv > 32 || !q.build(n_qv, q_vlabels, n_qe, q_edges) || q.n_edges == 0) return -1;
+  Graph g;
+  for (uint32_t v = 0; v < n_v; v++) g.add_vertex(v, vlabels[v]);
+  if (g.vlabel.size() < n_v) { g.vlabel.resize(n_v, NOT_EXIST); g.nbr.resize(n_v); g.elab.resize(n_v); }
+  for (uint64_t i = 0; i < n_e; i++) {
+    uint32_t a = edges[3 * i], b = edges[3 * i + 1];
+    if (a < n_v && b < n_v && a != b) g.add_edge(a, b, edges[3 * i + 2]);
+  }
+  for (uint64_t i = 0; i < n_up; i++) {
+    const oracle_update& u = ups[i];
+    if (u.type == 'v') {
+      if (u.is_add) g.add_vertex(u.id1, u.label);
+      else if (u.id1 < g.vlabel.size()) {
+        std::vector<uint32_t> ns = g.nbr[u.id1];
+        for (uint32_t w : ns) g.remove_edge(u.id1, w);
+        g.vlabel[u.id1] = NOT_EXIST;
+      }
+      continue;
+    }
+    if (u.id1 >= g.vlabel.size() || u.id2 >= g.vlabel.size() || u.id1 == u.id2) continue;
+    if (u.is_add) g.add_edge(u.id1, u.id2, u.label); else g.remove_edge(u.id1, u.id2);
+  }
+  const size_t n = g.vlabel.size();
+  if (words * 64 < n) return -3;
+  std::vector<std::vector<char>> li0, li1, lit;
+  calig_levels(q, g, homo != 0, li0, li1);
+  if (li0_out) pack_bits(li0, words, li0_out);
+  if (li1_out) pack_bits(li1, words, li1_out);
+  if (lit_out) {
+    calig_fixpoint(q, g, homo != 0, lit);
+    pack_bits(lit, words, lit_out);
   }
   return (int)n;
 }

@@ -16,6 +16,7 @@
  *   - DAG root / SymBi DAG .............. matching/SymBi/symbi.cpp:113-238
  *   - TurboFlux spanning tree ........... matching/TurboFlux/turboflux.cpp:69-219
  *   - d1 / d2 candidate flags ........... matching/SymBi/symbi.cpp:259-349, 404-469
+ *   - CaLiG lighting after static filter  matching/Parallel_CaLiG/parallel_calig.cpp:337-429, 970-975
  *
  * Counts are the number of injective (unless homomorphism), label-preserving
  * embeddings of the query that contain the updated edge.  The match-set hash
@@ -88,6 +89,21 @@ int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const 
                  uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
                  uint64_t n_up, const oracle_update* ups, int algo, uint32_t* root, uint32_t* order,
                  uint32_t* parents, uint64_t words, uint64_t* d1, uint64_t* d2);
+
+/* CaLiG-style candidate flags on the graph after the first n_up updates, as
+ * [n_qv][words] bitsets (any output may be null):
+ *   li0: L(v) = L(u) and v has, per (vertex label, edge label) pair of u's
+ *        query edges, at least as many neighbours as u (one under homo);
+ *   li1: li0 and every query neighbour of u has an li0 neighbour of v;
+ *   lit: the lighting of the reference's CaLiG after static filtering
+ *        (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:337-429,
+ *        970-975): the greatest set where every lit (u, v) maps u's query
+ *        neighbours to distinct lit neighbours of v.
+ * lit is contained in li1.  Returns the number of data vertex ids. */
+int oracle_calig_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
+                       uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
+                       uint64_t n_up, const oracle_update* ups, int homo, uint64_t words, uint64_t* li0,
+                       uint64_t* li1, uint64_t* lit);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,10 @@ def lib() -> C.CDLL:
         _lib.oracle_initial_count.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                               C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
                                               C.POINTER(C.c_uint64)]
+        _lib.oracle_calig_index.restype = C.c_int
+        _lib.oracle_calig_index.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                            C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_uint64,
+                                            C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.oracle_index.restype = C.c_int
         _lib.oracle_index.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                       C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
@@ -144,6 +148,35 @@ def index(q_vlabels, q_edges, vlabels, edges, updates=None, *, algo: str = "symb
     bits = lambda a: np.unpackbits(a.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)  # noqa: E731
     par = [[p for p in range(len(qv)) if (int(parents[q]) >> p) & 1] for q in range(len(qv))]
     return {"root": int(root.value), "order": order.tolist(), "parents": par, "d1": bits(d1), "d2": bits(d2)}
+
+
+def calig_index(q_vlabels, q_edges, vlabels, edges, updates=None, *, homo: bool = False,
+                with_lit: bool = True) -> dict:
+    """CaLiG-style flags after the given updates: li0 / li1 (the two levels the
+    engine maintains) and lit (the reference CaLiG's lighting after static
+    filtering), as bool arrays of shape [n_qv, n_vertices]."""
+    qv = np.ascontiguousarray(q_vlabels, dtype=np.uint32)
+    qe = np.ascontiguousarray(q_edges, dtype=np.uint32).reshape(-1, 3)
+    vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+    e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
+    u = np.ascontiguousarray(updates if updates is not None else np.zeros(0, UPDATE_DTYPE), dtype=UPDATE_DTYPE)
+    nmax = len(vl)
+    for r in u:
+        if r["type"] == ord("v"):
+            nmax = max(nmax, int(r["id1"]) + 1)
+    words = (nmax + 63) // 64 + 1
+    li0 = np.zeros((len(qv), words), dtype=np.uint64)
+    li1 = np.zeros((len(qv), words), dtype=np.uint64)
+    lit = np.zeros((len(qv), words), dtype=np.uint64)
+    n = lib().oracle_calig_index(len(qv), _p(qv), len(qe), _p(qe), len(vl), _p(vl), len(e), _p(e), len(u), _p(u),
+                                 int(homo), words, _p(li0), _p(li1), _p(lit) if with_lit else 0)
+    if n < 0:
+        raise RuntimeError(f"oracle_calig_index failed: {n}")
+    bits = lambda a: np.unpackbits(a.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)  # noqa: E731
+    out = {"li0": bits(li0), "li1": bits(li1)}
+    if with_lit:
+        out["lit"] = bits(lit)
+    return out
 
 
 def parse_index_dump(text: str, n_vertices: int) -> dict:

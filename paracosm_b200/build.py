@@ -7,6 +7,7 @@ Outputs (git-ignored, but they travel with the working tree):
     paracosm_b200/_bin/csm            csm driver (reference command line) over the engine
     paracosm_b200/_bin/csm_serve      serving loop (standing queries, streamed updates, continuous batching)
     paracosm_b200/_bin/csm_gen        seeded workload generator
+    paracosm_b200/_bin/calig          the reference's CaLiG program (its formats and output) over the engine
     oracle/_build/                    CPU restatement used as the checker
     oracle/_ref/                      the reference compiled from its sources (checker / CPU baseline)
 """
@@ -73,8 +74,8 @@ def build_host(force: bool = False) -> None:
     BIN.mkdir(parents=True, exist_ok=True)
     common = [HOST / "graph_io.cpp"]
     gen = BIN / "csm_gen"
-    gen_src = [HOST / "csm_gen.cpp", HOST / "workload.cpp"] + common
-    if force or _stale(gen, gen_src + [HOST / "workload.h", HOST / "graph_io.h"]):
+    gen_src = [HOST / "csm_gen.cpp", HOST / "workload.cpp", HOST / "calig_io.cpp"] + common
+    if force or _stale(gen, gen_src + [HOST / "workload.h", HOST / "graph_io.h", HOST / "calig_io.h"]):
         _run([CXX, "-std=c++17", "-O3", "-fopenmp", "-o", str(gen)] + [str(s) for s in gen_src])
     link = ["-L", str(LIB), "-lcsmgpu", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN/../_lib"]
     srv = BIN / "csm_serve"
@@ -90,6 +91,12 @@ def build_host(force: bool = False) -> None:
         if force or _stale(drv, deps):
             _run([CXX, "-std=c++17", "-O3", "-I", str(ROOT / "include"), "-o", str(drv)] + [str(s) for s in drv_src]
                  + ["-L", str(LIB), "-lcsmgpu", f"-Wl,-rpath,{LIB}", "-Wl,-rpath,$ORIGIN/../_lib"])
+    cal = BIN / "calig"
+    cal_src = [HOST / "calig_main.cpp", HOST / "calig_io.cpp", HOST / "plugins.cpp"] + common
+    deps = cal_src + [HOST / "calig_io.h", HOST / "plugins.h", HOST / "graph_io.h", ROOT / "include" / "csm_gpu.h",
+                      LIB / "libcsmgpu.so"]
+    if force or _stale(cal, deps):
+        _run([CXX, "-std=c++17", "-O3", "-I", str(ROOT / "include"), "-o", str(cal)] + [str(s) for s in cal_src] + link)
 
 
 def build_oracle(force: bool = False) -> None:

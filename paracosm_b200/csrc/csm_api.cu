@@ -423,7 +423,8 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, o->d_info, g, q->d_plan, q->index.d2, q->index.words,
                                               q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error,
                                               q->cfg.shard_rank, q->cfg.shard_count,
-                                              (uint32_t)q->cfg.turboflux_compat); CKL();
+                                              (uint32_t)q->cfg.turboflux_compat,
+                                              q->cfg.algorithm == CSM_ALGO_CALIG ? 1u : 0u); CKL();
   SearchParams sp{};
   sp.g = g; sp.plan = q->d_plan; sp.tasks = q->d_tasks; sp.n_tasks = c + 6; sp.task_cap = q->task_cap;
   sp.task_next = c + 7; sp.info = o->d_info; sp.count = q->d_count; sp.hash = q->d_hash; sp.bytes = q->d_bytes;
@@ -1094,7 +1095,8 @@ const char* csm_gpu_strerror(int code) {
 
 int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   if (!cfg || !out) return set_err(CSM_EINVAL, "null argument");
-  if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
+  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_CALIG)
+    return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
   if (cfg->shard_count > 1 && cfg->shard_rank >= cfg->shard_count)
     return set_err(CSM_EINVAL, "shard_rank %u outside shard_count %u", cfg->shard_rank, cfg->shard_count);
@@ -1219,7 +1221,8 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
   if (!owner || !cfg || !out || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
   if (owner->owner) return set_err(CSM_ESTATE, "attach to the context that owns the graph");
   if (!owner->has_graph || !owner->has_plan) return set_err(CSM_ESTATE, "the owner needs a graph and a built index");
-  if (cfg->algorithm < 0 || cfg->algorithm > 2) return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
+  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_CALIG)
+    return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   CK(cudaSetDevice(owner->dev));
   CK(cudaStreamSynchronize(owner->st));
   csm_ctx* a = new csm_ctx();
@@ -1269,7 +1272,7 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
     std::vector<std::vector<uint32_t>> qel_f(a->nq);
     for (uint32_t u = 0; u < a->nq; u++)
       for (uint32_t l : a->qel[u]) qel_f[u].push_back(fold_host(a->qlab_e, l));
-    IndexQuery q{a->nq, &a->qvl_f, &a->qnbr, &qel_f};
+    IndexQuery q{a->nq, &a->qvl_f, &a->qnbr, &qel_f, a->cfg.homomorphism != 0};
     rc = index_build(a->index, a->mem, a->g, q, a->cfg.algorithm, a->sm_count, a->st, &a->launches);
   }
   if (rc) return fail(rc);
@@ -1404,7 +1407,7 @@ int csm_gpu_build_index(csm_ctx* ctx) {
   std::vector<std::vector<uint32_t>> qel_f(ctx->nq);
   for (uint32_t u = 0; u < ctx->nq; u++)
     for (uint32_t l : ctx->qel[u]) qel_f[u].push_back(fold_host(ctx->qlab_e, l));
-  IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &qel_f};
+  IndexQuery q{ctx->nq, &ctx->qvl_f, &ctx->qnbr, &qel_f, ctx->cfg.homomorphism != 0};
   rc = index_build(ctx->index, ctx->mem, ctx->g, q, ctx->cfg.algorithm, ctx->sm_count, ctx->st, &ctx->launches);
   if (rc || !ctx->cfg.turboflux_compat) return rc;
   // compat deletions need to know which anchors are spanning-tree edges

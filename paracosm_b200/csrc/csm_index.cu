@@ -39,6 +39,13 @@ __device__ __forceinline__ bool lane_support(const uint32_t* pool, uint64_t lo, 
   return false;
 }
 
+// Entries of v in combo c (the union graph's segment during a batch).
+__device__ __forceinline__ uint64_t seg_count(const DevGraph& g, uint32_t v, uint32_t c) {
+  uint64_t lo, hi;
+  segment(g, v, c, lo, hi);
+  return hi - lo;
+}
+
 // The same over the whole warp (every lane must call it with equal arguments).
 __device__ __forceinline__ bool warp_support(const uint32_t* pool, uint64_t lo, uint64_t hi, const uint64_t* flag,
                                              uint32_t lane) {
@@ -129,7 +136,7 @@ __global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
   for (uint32_t s = 0; s < nsrc; s++) {
     const uint32_t q = phase == 1 ? dag->par[u][s] : dag->chd[u][s];
     const uint32_t combo = phase == 1 ? dag->par_ucombo[u][s] : dag->chd_ucombo[u][s];
-    const uint64_t* src = (phase == 1 ? b.c1 : b.c2) + (uint64_t)q * b.words;
+    const uint64_t* src = (phase == 1 || dag->lighting ? b.c1 : b.c2) + (uint64_t)q * b.words;
     for (uint64_t wi = warp; wi < b.words; wi += nwarps) {
       uint64_t word = src[wi];
       while (word) {
@@ -163,6 +170,10 @@ __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
   uint64_t* chg = (phase == 1 ? b.c1 : b.c2) + off;
   const uint64_t* d1u = b.d1 + off;
   const uint32_t nchk = phase == 1 ? dag->npar[u] : dag->nchd[u];
+  // support flags of the checked neighbours: d1 of parents; d2 of children,
+  // or their d1 in lighting mode
+  const uint64_t* sup = (phase == 1 || dag->lighting) ? b.d1 : b.d2;
+  const uint32_t nreq = (phase == 1 && dag->lighting) ? dag->nreq[u] : 0u;
   for (uint64_t wi = warp; wi < b.words; wi += nwarps) {
     uint64_t cand;
     if (full) {
@@ -196,10 +207,11 @@ __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
         bool long_seg = false;
         if (phase == 1) ok = g.vlabel[v] == lu;
         else ok = bit_of(d1u, v);
+        for (uint32_t r = 0; r < nreq && ok; r++) ok = seg_count(g, v, dag->req_combo[u][r]) >= dag->req_mult[u][r];
         for (uint32_t s = 0; s < nchk && ok; s++) {
           const uint32_t q = phase == 1 ? dag->par[u][s] : dag->chd[u][s];
           const uint32_t combo = phase == 1 ? dag->par_vcombo[u][s] : dag->chd_vcombo[u][s];
-          const uint64_t* flag = (phase == 1 ? b.d1 : b.d2) + (uint64_t)q * b.words;
+          const uint64_t* flag = sup + (uint64_t)q * b.words;
           uint64_t lo, hi;
           segment(g, v, combo, lo, hi);
           if (hi - lo > kLaneScanMax) { long_seg = true; break; }
@@ -217,10 +229,11 @@ __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
       defer &= defer - 1;
       const uint32_t v = (uint32_t)(wi * 64 + bitpos);
       bool ok = phase == 1 ? (g.vlabel[v] == lu) : bit_of(d1u, v);
+      for (uint32_t r = 0; r < nreq && ok; r++) ok = seg_count(g, v, dag->req_combo[u][r]) >= dag->req_mult[u][r];
       for (uint32_t s = 0; s < nchk && ok; s++) {
         const uint32_t q = phase == 1 ? dag->par[u][s] : dag->chd[u][s];
         const uint32_t combo = phase == 1 ? dag->par_vcombo[u][s] : dag->chd_vcombo[u][s];
-        const uint64_t* flag = (phase == 1 ? b.d1 : b.d2) + (uint64_t)q * b.words;
+        const uint64_t* flag = sup + (uint64_t)q * b.words;
         uint64_t lo, hi;
         segment(g, v, combo, lo, hi);
         ok = warp_support(pool, lo, hi, flag, lane);
@@ -310,24 +323,19 @@ static int index_launch_round(IndexState& ix, const DevGraph& g, cudaStream_t st
   return CSM_OK;
 }
 
-int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery& q, int algo, int sm_count,
-                cudaStream_t st, uint64_t* launches) {
-  index_free(ix, mem);
-  ix.algo = algo;
-  ix.sm_count = sm_count > 0 ? sm_count : 148;
-  if (algo != CSM_ALGO_TURBOFLUX && algo != CSM_ALGO_SYMBI) return CSM_OK;
+// DAG of the TurboFlux / SymBi plugin: root from the device edge frequencies,
+// then the SymBi BFS orientation or the TurboFlux spanning tree.
+static int dag_for(const IndexQuery& q, const DevGraph& g, int algo,
+                   const std::vector<std::pair<uint32_t, uint32_t>>& edges, const std::vector<uint32_t>& e_lab,
+                   int sm_count, DevMem& mem, cudaStream_t st, uint64_t* launches, uint32_t& root,
+                   std::vector<std::vector<uint32_t>>& par, std::vector<std::vector<uint32_t>>& chd,
+                   std::vector<std::vector<uint32_t>>& par_l, std::vector<std::vector<uint32_t>>& chd_l,
+                   std::vector<uint32_t>& order) {
   const uint32_t nq = q.n;
   const auto& ql = *q.vlabels;
   const auto& nbr = *q.nbr;
   const auto& el = *q.elabel;
-  // query edges u < u' in adjacency order, as the frequency scan visits them
-  std::vector<std::pair<uint32_t, uint32_t>> edges;
-  std::vector<uint32_t> e_lab;
-  for (uint32_t u = 0; u < nq; u++)
-    for (size_t i = 0; i < nbr[u].size(); i++)
-      if (u < nbr[u][i]) { edges.emplace_back(u, nbr[u][i]); e_lab.push_back(el[u][i]); }
   const uint32_t ne = (uint32_t)edges.size();
-  if (ne == 0 || ne > kMaxQE || nq > kMaxQ) return set_err(CSM_EUNSUPPORTED, "query size outside the index limits");
   // frequencies on the device
   std::vector<uint32_t> h_eu(ne), h_ec(ne), h_el(ne);
   for (uint32_t i = 0; i < ne; i++) {
@@ -345,7 +353,7 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   IXCK(cudaMemcpyAsync(d_e + ne, h_ec.data(), 4ull * ne, cudaMemcpyHostToDevice, st));
   IXCK(cudaMemcpyAsync(d_e + 2 * ne, h_el.data(), 4ull * ne, cudaMemcpyHostToDevice, st));
   IXCK(cudaMemsetAsync(d_f, 0, 8ull * (ne + kMaxQ + 1), st));
-  k_ix_freq<<<ix.sm_count * 4, 256, 0, st>>>(g, ne, d_e, d_e + ne, d_e + 2 * ne, d_f, d_f + ne);
+  k_ix_freq<<<sm_count * 4, 256, 0, st>>>(g, ne, d_e, d_e + ne, d_e + 2 * ne, d_f, d_f + ne);
   (*launches)++;
   IXCK(cudaGetLastError());
   std::vector<unsigned long long> freq(ne + kMaxQ + 1);
@@ -355,11 +363,9 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   mem.release(d_f, 8ull * (ne + kMaxQ + 1));
   std::vector<unsigned long long> lcount(freq.begin() + ne, freq.end());
   freq.resize(ne);
-  const uint32_t root = choose_root(q, edges, freq, lcount);
+  root = choose_root(q, edges, freq, lcount);
 
   // the DAG: parents / children with edge labels
-  std::vector<std::vector<uint32_t>> par(nq), chd(nq), par_l(nq), chd_l(nq);
-  std::vector<uint32_t> order;
   auto ffreq = [&](uint32_t a, uint32_t b) {
     const uint32_t x = std::min(a, b), y = std::max(a, b);
     for (uint32_t i = 0; i < ne; i++)
@@ -418,8 +424,18 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
     for (size_t h = 0; h < order.size(); h++)
       for (uint32_t w : chd[order[h]]) order.push_back(w);
   }
-  if (order.size() != nq) return set_err(CSM_EINVAL, "query graph is not connected");
+  return CSM_OK;
+}
 
+
+// Device DAG, flag bitsets and the full first evaluation.
+static int index_finish(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery& q, int algo, uint32_t root,
+                        const std::vector<uint32_t>& order, const std::vector<std::vector<uint32_t>>& par,
+                        const std::vector<std::vector<uint32_t>>& chd, const std::vector<std::vector<uint32_t>>& par_l,
+                        const std::vector<std::vector<uint32_t>>& chd_l, cudaStream_t st, uint64_t* launches) {
+  const uint32_t nq = q.n;
+  const auto& ql = *q.vlabels;
+  int rc = CSM_OK;
   IxDag& D = ix.h_dag;
   memset(&D, 0, sizeof(D));
   D.nq = nq;
@@ -441,6 +457,19 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
       D.ep[D.n_edges] = (uint8_t)u; D.ec[D.n_edges] = (uint8_t)c; D.eel[D.n_edges] = (uint16_t)l;
       D.n_edges++;
     }
+  }
+  if (algo == CSM_ALGO_CALIG) {
+    // d1 requirements: per (vertex label, edge label) pair of u's query
+    // edges, as many neighbours as u has of that pair (one under homo)
+    D.lighting = 1;
+    for (uint32_t u = 0; u < nq; u++)
+      for (size_t i = 0; i < chd[u].size(); i++) {
+        const uint16_t combo = D.chd_vcombo[u][i];
+        uint32_t r = 0;
+        while (r < D.nreq[u] && D.req_combo[u][r] != combo) r++;
+        if (r == D.nreq[u]) { D.req_combo[u][r] = combo; D.req_mult[u][r] = 0; D.nreq[u]++; }
+        if (!q.homo || D.req_mult[u][r] == 0) D.req_mult[u][r]++;
+      }
   }
   ix.root = root;
   ix.order = order;
@@ -472,6 +501,44 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   if (rc) return rc;
   IXCK(cudaStreamSynchronize(st));
   return CSM_OK;
+}
+
+int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery& q, int algo, int sm_count,
+                cudaStream_t st, uint64_t* launches) {
+  index_free(ix, mem);
+  ix.algo = algo;
+  ix.sm_count = sm_count > 0 ? sm_count : 148;
+  if (algo != CSM_ALGO_TURBOFLUX && algo != CSM_ALGO_SYMBI && algo != CSM_ALGO_CALIG) return CSM_OK;
+  const uint32_t nq = q.n;
+  const auto& ql = *q.vlabels;
+  const auto& nbr = *q.nbr;
+  const auto& el = *q.elabel;
+  // query edges u < u' in adjacency order, as the frequency scan visits them
+  std::vector<std::pair<uint32_t, uint32_t>> edges;
+  std::vector<uint32_t> e_lab;
+  for (uint32_t u = 0; u < nq; u++)
+    for (size_t i = 0; i < nbr[u].size(); i++)
+      if (u < nbr[u][i]) { edges.emplace_back(u, nbr[u][i]); e_lab.push_back(el[u][i]); }
+  const uint32_t ne = (uint32_t)edges.size();
+  if (ne == 0 || ne > kMaxQE || nq > kMaxQ) return set_err(CSM_EUNSUPPORTED, "query size outside the index limits");
+  if (algo == CSM_ALGO_CALIG && 2 * ne > kMaxQE)
+    return set_err(CSM_EUNSUPPORTED, "query has more than %u edges (lighting filter limit)", kMaxQE / 2);
+  std::vector<std::vector<uint32_t>> par(nq), chd(nq), par_l(nq), chd_l(nq);
+  std::vector<uint32_t> order;
+  uint32_t root = 0;
+  if (algo == CSM_ALGO_CALIG) {
+    // lighting: every query neighbour is a child, nobody has a parent
+    for (uint32_t u = 0; u < nq; u++) {
+      order.push_back(u);
+      for (size_t i = 0; i < nbr[u].size(); i++) { chd[u].push_back(nbr[u][i]); chd_l[u].push_back(el[u][i]); }
+    }
+  } else {
+    const int rc = dag_for(q, g, algo, edges, e_lab, ix.sm_count, mem, st, launches, root, par, chd, par_l, chd_l,
+                           order);
+    if (rc) return rc;
+  }
+  if (order.size() != nq) return set_err(CSM_EINVAL, "query graph is not connected");
+  return index_finish(ix, mem, g, q, algo, root, order, par, chd, par_l, chd_l, st, launches);
 }
 
 int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,

@@ -15,7 +15,18 @@
 // in L2.  Maintenance recomputes the flags only where they can change:
 // endpoints of changed edges, and neighbours (through the label-partitioned
 // CSR) of vertices whose flag changed at a DAG neighbour, level by level in
-// DAG order.  Every batch first brings the flags to the batch's union graph
+// DAG order.
+//
+// The CaLiG-style plugin uses the same machinery for its lighting filter
+// (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:337-429): the
+// "DAG" has no parents and makes every query neighbour a child, d1 is the
+// label test plus, per (vertex label, edge label) pair of u's query edges, at
+// least as many neighbours of that pair as u has (CaLiG's distinct witnesses
+// for same-label neighbours, counted), and d2 is d1 with every query
+// neighbour supported by a d1 neighbour.  Both levels are functions of the
+// graph, monotone in its edges, and contain the reference's lighting.
+//
+// Every batch first brings the flags to the batch's union graph
 // (a superset of the graph any of its updates sees, and the flags are
 // monotone in the edge set, so d2 stays a sound filter for all of them), and
 // to the graph after the batch once its deletions are applied.
@@ -32,6 +43,7 @@ struct IndexQuery {
   const std::vector<uint32_t>* vlabels;            // folded query vertex labels
   const std::vector<std::vector<uint32_t>>* nbr;   // sorted adjacency
   const std::vector<std::vector<uint32_t>>* elabel;  // folded edge labels, parallel to nbr
+  bool homo = false;  // homomorphism: the lighting filter asks one neighbour per (label, edge label) pair
 };
 
 // Query DAG in device memory.
@@ -47,6 +59,12 @@ struct IxDag {
   uint16_t chd_ucombo[kMaxQ][kMaxQ];  // combo (L(u), l(u,c))
   uint8_t ep[kMaxQE], ec[kMaxQE];    // DAG edge list: parent, child
   uint16_t eel[kMaxQE];              // folded edge label
+  // lighting mode: d2 draws its support from the children's d1, and d1
+  // requires req_mult[u][i] neighbours in combo req_combo[u][i]
+  uint32_t lighting;
+  uint32_t nreq[kMaxQ];
+  uint16_t req_combo[kMaxQ][kMaxQ];
+  uint8_t req_mult[kMaxQ][kMaxQ];
 };
 
 // Flag bitsets: [n_q][words] each.  m1 / m2 mark vertices to re-evaluate,

@@ -223,6 +223,7 @@ struct UpdInfo {
   uint32_t label;      // anchor label used for counting (existing label for deletions)
   uint32_t flags;      // bit0 valid edge update, bit1 insertion, bit2 mutation applied, bit3 invalid
 };
-enum : uint32_t { UF_VALID = 1u, UF_ADD = 2u, UF_MUT = 4u, UF_INVALID = 8u };
+// UF_DUP: an insertion of an edge that is present at that point of the batch
+enum : uint32_t { UF_VALID = 1u, UF_ADD = 2u, UF_MUT = 4u, UF_INVALID = 8u, UF_DUP = 16u };
 
 }  // namespace csm

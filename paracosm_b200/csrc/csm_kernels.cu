@@ -182,6 +182,7 @@ __global__ void k_resolve(const uint64_t* skey, const uint32_t* sseq, uint32_t B
     if (inf.flags & UF_ADD) {
       if (cur_p) {
         inf.label = label;  // duplicate insert: graph unchanged, counted with the given label
+        inf.flags |= UF_DUP;
       } else {
         cur_p = true; cur_l = label; cur_s = (int32_t)s;
         inf.label = label; inf.flags |= UF_MUT;

@@ -143,7 +143,7 @@ struct SearchParams {
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
                        uint32_t* safe, unsigned int* error, uint32_t shard_rank = 0, uint32_t shard_count = 1,
-                       uint32_t turboflux_compat = 0);
+                       uint32_t turboflux_compat = 0, uint32_t dup_zero = 0);
 size_t search_smem_bytes(uint32_t n_q, uint32_t warps);
 uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, bool with_enum = false);
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);

@@ -46,12 +46,14 @@ __device__ __forceinline__ bool d2_bit(const uint64_t* d2, uint64_t words, uint3
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,
                        uint32_t* safe, unsigned int* error, uint32_t shard_rank, uint32_t shard_count,
-                       uint32_t turboflux_compat) {
+                       uint32_t turboflux_compat, uint32_t dup_zero) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
   uint32_t sf = 1;
-  if ((u.flags & UF_VALID) && !(u.flags & UF_INVALID)) {
+  // dup_zero: an insertion of a present edge counts nothing (CaLiG skips it,
+  // ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:1233)
+  if ((u.flags & UF_VALID) && !(u.flags & UF_INVALID) && !(dup_zero && (u.flags & UF_DUP))) {
     const uint32_t L1 = g.vlabel[u.v1], L2 = g.vlabel[u.v2], l = u.label;
     const uint32_t na = plan->n_anchor;
     // The reference's TurboFlux deletion seeds every query edge whose vertex

@@ -386,6 +386,12 @@ class Parrllel_SymBi(_ParallelMixin, SymBi):
     ALGO = "parallel_symbi"
 
 
+class Parallel_CaLiG(_ParallelMixin, matching):
+    """CaLiG's candidate-lighting plugin (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp), which the
+    reference ships as its own program.  An insertion of a present edge counts 0."""
+    ALGO = "parallel_calig"
+
+
 PLUGINS = {
     "graphflow": Graphflow,
     "turboflux": TurboFlux,
@@ -393,4 +399,6 @@ PLUGINS = {
     "parallel_graphflow": Parallel_Graphflow,
     "parallel_turboflux": Parallel_TurboFlux,
     "parallel_symbi": Parrllel_SymBi,
+    "parallel_calig": Parallel_CaLiG,
+    "calig": Parallel_CaLiG,
 }

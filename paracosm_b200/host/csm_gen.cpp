@@ -1,13 +1,15 @@
 // csm_gen: writes a seeded synthetic workload (data graph, update stream,
 // queries) in the reference's text formats and/or the binary containers.
 //
-//   csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--no-binary]
+//   csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--calig] [--no-binary]
 //           [--log2-n K] [--avg-degree D] [--vlabels L] [--zipf S] [--elabels L]
 //           [--updates N] [--insert-frac F] [--holdout-frac F]
 //           [--query SIZE:dense|sparse[:EXTRA[:MINDEG]]] (repeatable; replaces the preset's)
 //
 // DIR receives data.bin / stream.bin (binary), data.graph / stream.txt (text,
-// with --text), query_<i>.graph, and meta.txt (the spec and sizes).
+// with --text), query_<i>.graph, and meta.txt (the spec and sizes).  --calig
+// also writes data.calig / stream.calig / query_<i>.calig in the reference
+// CaLiG program's formats (no edge labels; deletions as negative ids).
 #include <sys/stat.h>
 
 #include <chrono>
@@ -16,13 +18,14 @@
 #include <cstring>
 #include <string>
 
+#include "calig_io.h"
 #include "workload.h"
 
 using namespace csm;
 
 static void usage() {
   fprintf(stderr,
-          "csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--no-binary]\n"
+          "csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--calig] [--no-binary]\n"
           "        [--log2-n K] [--avg-degree D] [--vlabels L] [--zipf S] [--elabels L]\n"
           "        [--updates N] [--insert-frac F] [--holdout-frac F]\n"
           "        [--query SIZE:dense|sparse[:EXTRA[:MINDEG]]]...\n");
@@ -32,7 +35,7 @@ int main(int argc, char** argv) {
   WorkloadSpec s;
   preset("c1", s);
   std::string out;
-  bool text = false, binary = true, queries_set = false;
+  bool text = false, calig = false, binary = true, queries_set = false;
   for (int i = 1; i < argc; i++) {
     std::string k = argv[i];
     auto nxt = [&]() -> std::string { if (i + 1 >= argc) { usage(); exit(2); } return argv[++i]; };
@@ -40,6 +43,7 @@ int main(int argc, char** argv) {
     else if (k == "--out") out = nxt();
     else if (k == "--seed") s.seed = std::stoull(nxt());
     else if (k == "--text") text = true;
+    else if (k == "--calig") calig = true;
     else if (k == "--no-binary") binary = false;
     else if (k == "--log2-n") s.log2_n = (uint32_t)std::stoul(nxt());
     else if (k == "--avg-degree") s.avg_degree = std::stod(nxt());
@@ -79,6 +83,17 @@ int main(int argc, char** argv) {
   }
   for (size_t i = 0; i < w.queries.size(); i++)
     ok &= save_query_text(out + "/query_" + std::to_string(i) + ".graph", w.queries[i]);
+  if (calig) {
+    ok &= save_calig_graph(out + "/data.calig", w.initial);
+    ok &= save_calig_stream(out + "/stream.calig", w.stream);
+    for (size_t i = 0; i < w.queries.size(); i++) {
+      EdgeList q;
+      q.n = w.queries[i].n;
+      q.vlabels = w.queries[i].vlabels;
+      q.edges = w.queries[i].edges;
+      ok &= save_calig_graph(out + "/query_" + std::to_string(i) + ".calig", q);
+    }
+  }
   FILE* f = fopen((out + "/meta.txt").c_str(), "w");
   if (f) {
     fprintf(f, "name=%s\nseed=%llu\nlog2_n=%u\navg_degree=%g\nrmat=%g,%g,%g\nvlabels=%u\nzipf=%g\nelabels=%u\n",

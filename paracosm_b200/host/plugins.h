@@ -7,6 +7,8 @@
 //   parallel_graphflow, graphflow  -> CSM_ALGO_GRAPHFLOW (no index)
 //   parallel_turboflux, turboflux  -> CSM_ALGO_TURBOFLUX (DCG over a spanning tree)
 //   parallel_symbi, symbi          -> CSM_ALGO_SYMBI     (DCS over a DAG of all query edges)
+//   parallel_calig, calig          -> CSM_ALGO_CALIG     (CaLiG-style lighting filter; the reference
+//                                     ships CaLiG as its own program, matching/Parallel_CaLiG)
 // Differences from the reference, all deliberate:
 //   - errors never exit the process: the calls record a CSM_E* code, and
 //     error() / error_text() report the first one;
@@ -112,6 +114,16 @@ class Parrllel_SymBi : public matching {
   Parrllel_SymBi(const EdgeList& q, const EdgeList& d, size_t max_results, bool print_prep, bool print_enum,
                  bool homo, const GpuOptions& opt)
       : matching(q, d, max_results, print_prep, print_enum, homo, CSM_ALGO_SYMBI, opt) {}
+};
+
+// CaLiG (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp) is a
+// standalone program in the reference; behind this interface it takes the
+// same inputs as the other plugins.  An insertion of a present edge counts 0.
+class Parallel_CaLiG : public matching {
+ public:
+  Parallel_CaLiG(const EdgeList& q, const EdgeList& d, size_t max_results, bool print_prep, bool print_enum,
+                 bool homo, const GpuOptions& opt)
+      : matching(q, d, max_results, print_prep, print_enum, homo, CSM_ALGO_CALIG, opt) {}
 };
 
 // Plugin for an -a name, or nullptr for an unknown name.

@@ -82,6 +82,54 @@ def read_stream(path: str | os.PathLike) -> np.ndarray:
     return np.array(recs, dtype=UPDATE_DTYPE)
 
 
+def read_calig_graph(path: str | os.PathLike) -> tuple[np.ndarray, np.ndarray]:
+    """(vertex labels, (m, 3) edge triples with label 0) of a graph or query in the
+    reference CaLiG program's format (`v id label`, `e a b`;
+    ParaCOSM/CSM/matching/CaLiG/README.md).  As its inputQ / inputG
+    (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:101-143, 271-335):
+    a label of -1 reads as 0, and edges with an endpoint beyond the largest
+    vertex id are dropped.  Duplicate edges are kept once."""
+    toks = Path(path).read_text().split()
+    vl: list[int] = []
+    raw: list[tuple[int, int]] = []
+    i = 0
+    while i < len(toks):
+        if toks[i] == "v":
+            vid, lab = int(toks[i + 1]), int(toks[i + 2])
+            if vid >= len(vl):
+                vl.extend([NOT_EXIST] * (vid + 1 - len(vl)))
+            vl[vid] = max(lab, 0)
+        elif toks[i] == "e":
+            raw.append((int(toks[i + 1]), int(toks[i + 2])))
+        else:
+            raise ValueError(f"unexpected token {toks[i]!r} in {path}")
+        i += 3
+    seen, edges = set(), []
+    for a, b in raw:
+        if a < 0 or b < 0 or a >= len(vl) or b >= len(vl) or a == b:
+            continue
+        k = (min(a, b), max(a, b))
+        if k not in seen:
+            seen.add(k)
+            edges.append((a, b, 0))
+    return np.array(vl, dtype=np.uint32), np.array(edges, dtype=np.uint32).reshape(-1, 3)
+
+
+def read_calig_stream(path: str | os.PathLike) -> np.ndarray:
+    """Update records of a CaLiG stream: `e a b` inserts (a, b), `e -a-1 -b-1` deletes it."""
+    toks = Path(path).read_text().split()
+    recs = []
+    for i in range(0, len(toks) - 2, 3):
+        a, b = int(toks[i + 1]), int(toks[i + 2])
+        if a < 0 and b < 0:
+            recs.append((ord("e"), 0, 0, -a - 1, -b - 1, 0))
+        elif a >= 0 and b >= 0:
+            recs.append((ord("e"), 1, 0, a, b, 0))
+        else:
+            raise ValueError(f"mixed-sign edge record in {path}")
+    return np.array(recs, dtype=UPDATE_DTYPE)
+
+
 def write_graph_text(path: str | os.PathLike, vlabels: np.ndarray, edges: np.ndarray) -> None:
     with open(path, "w") as f:
         for v, l in enumerate(vlabels):

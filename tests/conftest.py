@@ -23,6 +23,24 @@ def golden_cases() -> list[str]:
     return sorted(d.name for d in GOLDEN.iterdir() if d.is_dir() and (d / "expected.csv").exists())
 
 
+def calig_cases() -> list[str]:
+    """Fixtures in the reference CaLiG program's formats, with its per-update counts."""
+    return sorted(d.name for d in GOLDEN.iterdir() if d.is_dir() and (d / "expected.txt").exists())
+
+
+def load_calig(name: str) -> dict:
+    from paracosm_b200 import workload
+    d = GOLDEN / name
+    qv, qe = workload.read_calig_graph(d / "query")
+    vl, e = workload.read_calig_graph(d / "data")
+    s = workload.read_calig_stream(d / "stream")
+    exp = np.loadtxt(d / "expected.txt", dtype=np.uint64).reshape(-1)
+    lit_pairs = np.loadtxt(d / "lit.txt", dtype=np.int64).reshape(-1, 2)
+    lit = np.zeros((len(qv), len(vl)), dtype=bool)
+    lit[lit_pairs[:, 0], lit_pairs[:, 1]] = True
+    return {"dir": d, "qv": qv, "qe": qe, "vl": vl, "e": e, "stream": s, "exp": exp, "lit": lit}
+
+
 def load_golden(name: str) -> dict:
     from paracosm_b200 import workload
     d = GOLDEN / name

@@ -17,6 +17,14 @@ before the stream.
     python tests/golden/make_golden.py          # needs the reference sources to build the driver
     python tests/golden/make_golden.py --index  # only the index fixtures
     python tests/golden/make_golden.py --initial  # only initial.json (InitialMatching counts of csm)
+    python tests/golden/make_golden.py --calig    # only the calig_* cases
+
+The calig_* cases are in the reference CaLiG program's own formats (data,
+query, stream; no edge labels, insertions only, since the reference cannot
+process deletion records) and hold, per update, the count of the
+reference's CaLiG (oracle/_ref/calig_ref, its update loop run serially) in
+expected.txt, and the lighting after its static filtering in lit.txt (one
+`u v` pair per lit candidate).
 
 Only this script reads the reference; the fixtures it writes are plain files.
 """
@@ -82,6 +90,47 @@ def write_index(d: Path) -> None:
 
 
 REF_CSM = ROOT / "oracle" / "_ref" / "csm"
+REF_CALIG = ROOT / "oracle" / "_ref" / "calig_ref"
+
+# name: generator args (one edge label, insertions only)
+CALIG_CASES = {
+    # several insertions at vertices that had no neighbour in the initial graph
+    "calig_sparse": ["--preset", "c2", "--log2-n", "10", "--avg-degree", "6", "--vlabels", "3", "--zipf", "0",
+                     "--elabels", "1", "--updates", "300", "--insert-frac", "1.0", "--seed", "1",
+                     "--query", "5:sparse:1"],
+    "calig_dense": ["--preset", "c2", "--log2-n", "11", "--avg-degree", "10", "--vlabels", "2", "--zipf", "0",
+                    "--elabels", "1", "--updates", "300", "--insert-frac", "1.0", "--seed", "7",
+                    "--query", "6:dense"],
+    "calig_tree": ["--preset", "c2", "--log2-n", "10", "--avg-degree", "8", "--vlabels", "4", "--zipf", "0",
+                   "--elabels", "1", "--updates", "400", "--insert-frac", "1.0", "--seed", "27",
+                   "--query", "6:sparse:2"],
+    # from update 97 on the reference counts fewer matches than exist: a vertex
+    # without neighbours in the initial graph keeps partial candidate maps,
+    # which its later insertions do not fill (kept as a record of that defect)
+    "calig_undercount": ["--preset", "c2", "--log2-n", "10", "--avg-degree", "4", "--vlabels", "2", "--zipf", "0",
+                         "--elabels", "1", "--updates", "400", "--insert-frac", "1.0", "--seed", "40",
+                         "--query", "5:sparse:1"],
+}
+
+
+def write_calig(name: str, args: list[str]) -> None:
+    d = HERE / name
+    tmp = HERE / f"_tmp_{name}"
+    if tmp.exists():
+        shutil.rmtree(tmp)
+    subprocess.run([str(GEN)] + args + ["--out", str(tmp), "--calig", "--no-binary"], check=True, capture_output=True)
+    d.mkdir(exist_ok=True)
+    shutil.copy(tmp / "data.calig", d / "data")
+    shutil.copy(tmp / "stream.calig", d / "stream")
+    shutil.copy(tmp / "query_0.calig", d / "query")
+    shutil.rmtree(tmp)
+    r = subprocess.run([str(REF_CALIG), "-d", "data", "-q", "query", "-s", "stream", "--out", "expected.txt",
+                        "--dump-li", "lit.txt"], cwd=d, capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(f"{name}: calig_ref failed: {r.stderr[-400:]}")
+    (d / "params.json").write_text(json.dumps({"generator": args, "reference": "ParaCOSM/CSM/matching/"
+                                               "Parallel_CaLiG/parallel_calig.cpp, serial"}, indent=1) + "\n")
+    print(name, r.stderr.strip().splitlines()[-1])
 
 
 def write_initial(d: Path, homo: bool) -> None:
@@ -98,6 +147,10 @@ def write_initial(d: Path, homo: bool) -> None:
 
 
 def main() -> None:
+    if "--calig" in sys.argv:
+        for name, args in CALIG_CASES.items():
+            write_calig(name, args)
+        return
     if "--initial" in sys.argv:
         for name, (_, _, homo) in CASES.items():
             write_initial(HERE / name, homo)
