@@ -377,6 +377,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the search-shape autotuner")
+    ap.add_argument("--tail-enumerate", action="store_true",
+                    help="enumerate the independent tail of each order instead of counting it")
     ap.add_argument("--serve-rates", default="1e4,1e5,1e6",
                     help="offered loads (updates/s) for the serving-loop leg; empty to skip")
     ap.add_argument("--serve-seconds", type=float, default=4.0)
@@ -418,8 +420,9 @@ def main():
     t0 = time.perf_counter()
     # N > 1: every rank holds a replica and applies every batch; root tasks are dealt
     # across ranks and one all-reduce per batch combines the per-update results
+    te = bool(args.tail_enumerate)
     eng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev,
-                 shard_rank=rank if world > 1 else 0, shard_count=world)
+                 shard_rank=rank if world > 1 else 0, shard_count=world, tail_enumerate=te)
     eng.set_query(qv, qe)
     eng.load_graph(w.vlabels, w.edges)
     eng.build_index()
@@ -481,7 +484,7 @@ def main():
     # timed region starts with) ----
     kw = {k: shape[k] for k in ("warps_per_block", "blocks_per_sm", "donate_every", "split_deep")} if shape else {}
     eng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev,
-                 shard_rank=rank if world > 1 else 0, shard_count=world, **kw)
+                 shard_rank=rank if world > 1 else 0, shard_count=world, tail_enumerate=te, **kw)
     eng.set_query(qv, qe)
     eng.load_graph(w.vlabels, w.edges)
     eng.build_index()
@@ -517,7 +520,7 @@ def main():
     if rank == 0 and args.plain_sample > 0:
         P = min(args.plain_sample, len(stream))
         sample = np.ascontiguousarray(stream[:P])
-        beng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev)
+        beng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev, tail_enumerate=te)
         beng.set_query(qv, qe)
         beng.load_graph(w.vlabels, w.edges)
         beng.build_index()
@@ -526,7 +529,8 @@ def main():
         forms = {}
         for graphs in (True, False):
             kw = {k: shape[k] for k in ("warps_per_block", "blocks_per_sm", "donate_every", "split_deep")} if shape else {}
-            peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev, graphs=graphs, **kw)
+            peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev, graphs=graphs,
+                          tail_enumerate=te, **kw)
             peng.set_query(qv, qe)
             peng.load_graph(w.vlabels, w.edges)
             peng.build_index()
@@ -569,6 +573,7 @@ def main():
             "dtype": "u32", "data": "synthetic",
             "config": {"workload": cfg["workload"], "plugin": cfg["algo"], "batch": B, "updates_timed": K * B,
                        "search_shape": shape,
+                       "tail": "enumerated" if te else "counted (independent tail of each order)",
                        "l2": "inputs larger than L2 (graph ~1.2 GB in HBM)", "max_results": cfg["max_results"],
                        "parallelism": f"seed-sharded x{world} (replicated graph, one all-reduce per batch)"
                        if world > 1 else "single GPU"},

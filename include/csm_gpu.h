@@ -4,7 +4,8 @@
  * The engine replaces the hot path behind the reference's plugin interface
  * `class matching` (ParaCOSM/CSM/matching/matching.h:9-66) for the plugins
  * `parallel_graphflow`, `parallel_turboflux` and `parallel_symbi`
- * (ParaCOSM/CSM/matching/main.cpp:740-757).  A C++ host (paracosm_b200/host)
+ * (ParaCOSM/CSM/matching/main.cpp:740-757), and the reference's standalone
+ * CaLiG program (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp).  A C++ host (paracosm_b200/host)
  * wraps these entry points in `matching`-style plugin classes so that the
  * csm command line and its output lines are unchanged.
  *
@@ -95,7 +96,10 @@ typedef struct csm_cfg {
   uint32_t split_deep;        /* smallest driver range split deep in the search tree; 0 = autotuned / 64 */
   uint32_t enum_capacity;     /* > 0: keep up to this many embeddings of each submit (--print-enum,
                                  read with csm_gpu_matches); not with CSM_GRAPHS_ON */
-  uint32_t reserved[1];
+  uint32_t tail_enumerate;    /* when only counts are wanted (want_hash 0, no match sets) the search
+                                 counts the last positions of an order that share no query edge as a
+                                 product of candidate counts (not in the reference); != 0 enumerates
+                                 them one by one instead.  Counts are the same; work_bytes differ */
 } csm_cfg;
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */

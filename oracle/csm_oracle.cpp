@@ -165,6 +165,72 @@ void graphflow_orders(const QueryGraph& q, std::vector<std::vector<uint32_t>>& o
   }
 }
 
+// Independent tail of an order (the engine's counting search, not in the
+// reference): the longest suffix o[s..n-1], s >= 2, with no query edge inside
+// it and no vertex label more than kTailGroup times.  Every tail vertex has
+// all its neighbours before s, so given a match of o[0..s-1] the tail
+// vertices only interact through injectivity, which only binds vertices of
+// one label: the completions are the product over label groups of each
+// group's number of injective assignments.  Returns s - 1 (the last position
+// matched one by one) when the tail has at least two vertices, else 0.
+constexpr uint32_t kTailGroup = 3;
+
+uint32_t independent_tail(const QueryGraph& q, const std::vector<uint32_t>& o) {
+  const uint32_t n = q.n;
+  if (n < 4) return 0;
+  std::vector<int> pos(n);
+  for (uint32_t i = 0; i < n; i++) pos[o[i]] = (int)i;
+  uint32_t s = n - 1;
+  while (s > 2) {
+    const uint32_t u = o[s - 1];
+    bool stop = false;
+    for (uint32_t w : q.nbr[u]) if (pos[w] >= (int)s) stop = true;  // an edge into the tail
+    uint32_t same = 0;
+    for (uint32_t i = s; i < n; i++) same += q.vlabel[o[i]] == q.vlabel[u];
+    if (stop || same >= kTailGroup) break;
+    s--;
+  }
+  return n - s >= 2 ? s - 1 : 0;
+}
+
+// Number of injective assignments of a group of g members given, for each
+// nonempty membership set M (bit i: the element is a candidate of member i),
+// the number N[M] of elements with exactly that membership: members served by
+// elements of one class M are a subset R of M, in N[M] * (N[M]-1) * ... ways.
+// Without injectivity (homo) it is the product of the members' candidate
+// counts.  Saturates at kSat.
+uint64_t group_assignments(uint32_t g, const uint64_t* N, bool homo) {
+  const uint64_t kSat = 1ULL << 58;
+  auto mul = [&](uint64_t a, uint64_t b) { return (a == 0 || b == 0) ? 0 : (a > kSat / b ? kSat : std::min(kSat, a * b)); };
+  const uint32_t full = (1u << g) - 1;
+  if (homo) {
+    uint64_t prod = 1;
+    for (uint32_t i = 0; i < g; i++) {
+      uint64_t c = 0;
+      for (uint32_t M = 1; M <= full; M++) if (M >> i & 1) c = std::min(kSat, c + N[M]);
+      prod = mul(prod, c);
+    }
+    return prod;
+  }
+  uint64_t f[1u << kTailGroup] = {1};
+  for (uint32_t M = 1; M <= full; M++) {
+    if (!N[M]) continue;
+    uint64_t h[1u << kTailGroup] = {0};
+    for (uint32_t S = 0; S <= full; S++) {
+      if (!f[S]) continue;
+      const uint32_t free_ = M & ~S;
+      for (uint32_t R = free_;; R = (R - 1) & free_) {  // every subset R of free_, R = 0 included
+        uint64_t ways = 1;
+        for (uint32_t r = 0, k = (uint32_t)__builtin_popcount(R); r < k; r++) ways = mul(ways, N[M] - r);
+        if (ways) h[S | R] = std::min(kSat, h[S | R] + mul(f[S], ways));
+        if (R == 0) break;
+      }
+    }
+    for (uint32_t S = 0; S <= full; S++) f[S] = h[S];
+  }
+  return f[full];
+}
+
 struct Searcher {
   const QueryGraph& q;
   Graph& g;
@@ -175,12 +241,88 @@ struct Searcher {
   std::vector<char> visited;
   uint64_t count = 0, hash = 0, bytes = 0;
   bool capped = false;
+  // per order: last position matched one by one before the independent tail
+  // (0: no tail counting for that order)
+  std::vector<uint32_t> tail_at;
 
   Searcher(const QueryGraph& q_, Graph& g_, const std::vector<std::vector<uint32_t>>& o, bool h, bool wh, uint64_t c)
       : q(q_), g(g_), order(o), homo(h), want_hash(wh), cap(c) {}
 
+  // Is data vertex v a candidate of query vertex u under the current prefix
+  // (label, adjacency with the edge label to every matched neighbour,
+  // injectivity against the prefix)?
+  bool is_candidate(uint32_t u, uint32_t v) {
+    if (g.label(v) != q.vlabel[u]) return false;
+    if (!homo && visited[v]) return false;
+    const auto& qn = q.nbr[u];
+    const auto& ql = q.elab[u];
+    for (size_t j = 0; j < qn.size(); j++) {
+      const uint32_t uo = qn[j];
+      if (m[uo] == NOT_EXIST) continue;
+      const auto& on = g.nbr[m[uo]];
+      auto it = std::lower_bound(on.begin(), on.end(), v);
+      if (it == on.end() || *it != v || g.elab[m[uo]][(size_t)(it - on.begin())] != ql[j]) return false;
+    }
+    return true;
+  }
+
+  // Candidates of query vertex u (scanning its smallest back neighbour's
+  // list); adds the node's algorithmic bytes.
+  void candidates(uint32_t u, std::vector<uint32_t>& out) {
+    out.clear();
+    const auto& qn = q.nbr[u];
+    const auto& ql = q.elab[u];
+    uint32_t u_min = NOT_EXIST, u_min_size = 0xffffffffu;
+    for (size_t i = 0; i < qn.size(); i++) {
+      if (m[qn[i]] == NOT_EXIST) continue;
+      const uint32_t sz = g.deg(m[qn[i]]);
+      if (sz < u_min_size) { u_min_size = sz; u_min = qn[i]; }
+      bytes += 4ULL * g.seg_size(m[qn[i]], q.vlabel[u], ql[i]);
+    }
+    for (uint32_t v : g.nbr[m[u_min]])
+      if (is_candidate(u, v)) out.push_back(v);
+  }
+
+  // The independent tail (independent_tail) from position `first` on: label
+  // groups in order of their first position, members in position order.  For
+  // each group, every member's candidates are listed (adding its bytes) and
+  // classified by membership in the group's other members; an element is
+  // counted once, under the first member it is a candidate of.  A group is
+  // only looked at while the product is nonzero.
+  void count_tail(uint32_t oi, uint32_t first) {
+    const uint64_t kSat = 1ULL << 58;
+    const auto& o = order[oi];
+    std::vector<char> done(q.n, 0);
+    uint64_t prod = 1;
+    std::vector<uint32_t> c;
+    for (uint32_t d = first; d < q.n && prod; d++) {
+      if (done[d]) continue;
+      std::vector<uint32_t> grp;
+      for (uint32_t e = d; e < q.n; e++)
+        if (!done[e] && q.vlabel[o[e]] == q.vlabel[o[d]]) { grp.push_back(e); done[e] = 1; }
+      uint64_t N[1u << kTailGroup] = {0};
+      for (uint32_t j = 0; j < grp.size(); j++) {
+        candidates(o[grp[j]], c);
+        for (uint32_t x : c) {
+          uint32_t M = 1u << j;
+          bool seen = false;
+          for (uint32_t i = 0; i < grp.size() && !seen; i++) {
+            if (i == j || !is_candidate(o[grp[i]], x)) continue;
+            if (i < j) seen = true; else M |= 1u << i;
+          }
+          if (!seen) N[M]++;
+        }
+      }
+      const uint64_t w = group_assignments((uint32_t)grp.size(), N, homo);
+      prod = w == 0 ? 0 : (prod > kSat / w ? kSat : std::min(kSat, prod * w));
+    }
+    count += prod;
+    if (cap && count >= cap) capped = true;
+  }
+
   // GraphFlow::FindMatches (graphflow.cpp:181-265)
   void find(uint32_t oi, uint32_t depth, uint64_t hsum) {
+    if (!tail_at.empty() && tail_at[oi] && depth == tail_at[oi] + 1) { count_tail(oi, depth); return; }
     const uint32_t u = order[oi][depth];
     const auto& qn = q.nbr[u];
     const auto& ql = q.elab[u];
@@ -298,7 +440,11 @@ extern "C" int oracle_run(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_q
   }
   std::vector<std::vector<uint32_t>> order;
   graphflow_orders(q, order);
+  std::vector<uint32_t> tail_at;
+  if (!want_hash)  // counting only: the tail of each order is counted, not enumerated
+    for (const auto& o : order) tail_at.push_back(independent_tail(q, o));
   Searcher s(q, g, order, homo != 0, want_hash != 0, max_results);
+  s.tail_at = tail_at;
   s.m.assign(n_qv, NOT_EXIST);
   s.visited.assign(g.vlabel.size(), 0);
 

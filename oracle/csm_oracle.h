@@ -26,6 +26,13 @@
  * sizes of all backward neighbour segments S(m[u_j], L(u), l(u,u_j)), in the
  * GraphFlow order of the anchor query edge, plus 16 B per applied edge
  * mutation.
+ *
+ * With want_hash = 0 the search is the engine's counting search: the
+ * independent tail of each order (the longest suffix with no query edge
+ * inside and no vertex label more than three times) is counted instead of
+ * being enumerated: a product over label groups of injective assignments.  Counts are the
+ * same; `bytes` then covers the nodes that search expands (each tail
+ * position once per prefix, while the product is nonzero).
  */
 #ifndef CSM_ORACLE_H
 #define CSM_ORACLE_H

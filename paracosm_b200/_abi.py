@@ -70,7 +70,7 @@ class CsmCfg(C.Structure):
         ("donate_every", C.c_uint32),
         ("split_deep", C.c_uint32),
         ("enum_capacity", C.c_uint32),
-        ("reserved", C.c_uint32 * 1),
+        ("tail_enumerate", C.c_uint32),
     ]
 
 

@@ -200,6 +200,39 @@ static uint32_t qedge_label(const csm_ctx* ctx, uint32_t a, uint32_t b) {
   return fold_host(ctx->qlab_e, ctx->qel[a][(size_t)(it - nb.begin())]);
 }
 
+// Independent tail of order o (PlanAnchor): the longest suffix o[s..n-1],
+// s >= 2, with no query edge inside and no vertex label more than kTailGroup
+// times; used when it has at least two vertices.
+static void plan_tail(const csm_ctx* ctx, const std::vector<uint32_t>& o, PlanAnchor& A) {
+  const uint32_t n = ctx->nq;
+  A.tail_at = 0; A.n_groups = 0; A.prefix_mask = 0xffffffffu;
+  if (n < 4) return;
+  std::vector<int> pos(n);
+  for (uint32_t i = 0; i < n; i++) pos[o[i]] = (int)i;
+  uint32_t s = n - 1;
+  while (s > 2) {
+    const uint32_t u = o[s - 1];
+    bool stop = false;
+    for (uint32_t w : ctx->qnbr[u]) if (pos[w] >= (int)s) stop = true;
+    uint32_t same = 0;
+    for (uint32_t i = s; i < n; i++) same += ctx->qvl_f[o[i]] == ctx->qvl_f[u];
+    if (stop || same >= kTailGroup) break;
+    s--;
+  }
+  if (n - s < 2) return;
+  A.tail_at = (uint8_t)(s - 1);
+  A.prefix_mask = (1u << s) - 1u;
+  std::vector<char> done(n, 0);
+  uint32_t k = 0;
+  for (uint32_t d = s; d < n; d++) {
+    if (done[d]) continue;
+    uint32_t g = 0;
+    for (uint32_t e = d; e < n; e++)
+      if (!done[e] && ctx->qvl_f[o[e]] == ctx->qvl_f[o[d]]) { done[e] = 1; A.gpos[k++] = (uint8_t)e; g++; }
+    A.gsize[A.n_groups++] = (uint8_t)g;
+  }
+}
+
 static int build_plan(csm_ctx* ctx) {
   std::vector<std::vector<uint32_t>> order;
   graphflow_orders(ctx, order);
@@ -229,6 +262,7 @@ static int build_plan(csm_ctx* ctx) {
       }
       if (pp.nb == 0) return set_err(CSM_EINVAL, "query graph is not connected");
     }
+    plan_tail(ctx, o, A);
   }
   ctx->plan_bytes = offsetof(Plan, anchors) + (size_t)P->n_anchor * sizeof(PlanAnchor);
   if (!ctx->d_plan) {
@@ -440,6 +474,7 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   sp.deadline_ns = q->cfg.deadline_ns;
   sp.donate_every = q->cfg.donate_every;
   sp.split_deep = q->cfg.split_deep;
+  sp.tail = (!q->cfg.want_hash && !q->d_enum && !q->cfg.tail_enumerate) ? 1u : 0u;
   if (q->d_enum) {
     sp.enum_buf = q->d_enum; sp.enum_n = q->d_enum_n; sp.enum_cap = q->cfg.enum_capacity;
     sp.enum_base = (uint32_t)(out - q->d_results);  // this batch's first update within the submit
@@ -893,6 +928,7 @@ static int tune_run(csm_ctx* ctx, uint32_t B, uint32_t warps, uint32_t bps, floa
   sp.sstat = ctx->d_sstat;
   sp.donate_every = donate_every;
   sp.split_deep = split_deep;
+  sp.tail = (!ctx->cfg.want_hash && !ctx->d_enum && !ctx->cfg.tail_enumerate) ? 1u : 0u;  // as the batches run
   CK(cudaEventRecord(ctx->ev_start, st));
   launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
   CK(cudaEventRecord(ctx->ev_end, st));
@@ -1053,6 +1089,7 @@ static int initial_match(csm_ctx* ctx, uint64_t* out) {
     sp.task_limit_ns = 20ull * 1000000000ull;
     sp.batch = B;
     sp.sstat = ctx->d_sstat;
+    sp.tail = ctx->cfg.tail_enumerate ? 0u : 1u;
     launch_search(sp, ctx->nq, (uint32_t)ctx->sm_count * bps, warps, st); CKL();
     ctx->search_launches++;
     k_init_sum<<<std::min<uint32_t>(blocks_for(B, 256), 1024), 256, 0, st>>>(B, ctx->d_count, total); CKL();
@@ -1229,6 +1266,7 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
   a->cfg = owner->cfg;
   a->cfg.algorithm = cfg->algorithm;
   a->cfg.max_results = cfg->max_results;
+  a->cfg.tail_enumerate = cfg->tail_enumerate;
   a->cfg.want_hash = cfg->want_hash;
   a->cfg.warps_per_block = cfg->warps_per_block;
   a->cfg.blocks_per_sm = cfg->blocks_per_sm;

@@ -195,9 +195,23 @@ struct PlanPos {
   uint32_t samelab;    // bitmask over earlier positions with the same label
 };
 
+// Independent tail of an order: positions tail_at + 1 .. n - 1 have no query
+// edge among them and no vertex label more than kTailGroup times, so once
+// positions 0 .. tail_at are matched the completions are a product over the
+// tail's label groups of injective assignments, counted without enumerating
+// them.  Groups are listed in order of their first position (gpos: the
+// positions, group after group, ascending inside a group; gsize: sizes).
+constexpr uint32_t kTailGroup = 3;
+
 struct PlanAnchor {
   uint32_t la, lb, el;       // label triple of the anchor (pos 0 label, pos 1 label, edge label)
   uint32_t tree;             // the anchor is an edge of the TurboFlux spanning tree (compat deletions)
+  uint32_t prefix_mask;      // positions 0 .. tail_at
+  uint8_t tail_at;           // last position matched one by one before the tail; 0: no tail
+  uint8_t n_groups;
+  uint8_t pad_[2];
+  uint8_t gsize[kMaxQ];
+  uint8_t gpos[kMaxQ];
   PlanPos pos[kMaxQ];
   uint8_t back_pos[kMaxQE];
   uint16_t back_combo[kMaxQE];

@@ -139,6 +139,9 @@ struct SearchParams {
   unsigned long long* enum_n;
   unsigned long long enum_cap;
   uint32_t enum_base, enum_stride;
+  // nonzero: count each anchor's independent tail (PlanAnchor::tail_at)
+  // instead of enumerating it; only for counts without hashes or match sets
+  uint32_t tail;
 };
 __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* plan, const uint64_t* d2,
                        uint64_t d2_words, Task* tasks, unsigned int* n_tasks, uint32_t task_cap,

@@ -99,10 +99,10 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
 // round trip to L2 serves up to four searches instead of one.
 __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uint32_t* pool, const PlanAnchor* A,
                                                 uint32_t pos, uint32_t x, const uint32_t* m, uint32_t dsel,
-                                                int32_t t) {
+                                                int32_t t, uint32_t lab_mask = 0xffffffffu) {
   const PlanPos P = A->pos[pos];
   if (!p.homo) {
-    for (uint32_t mk = P.samelab; mk; mk &= mk - 1) {
+    for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) {
       if (m[__ffs(mk) - 1] == x) return false;
     }
   }
@@ -208,7 +208,7 @@ struct TaskAcc {
 // donated task is a partial match (positions 0..L) plus a driver range for
 // position L + 1.  Returns the number of tasks handed over.
 __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t lane, uint32_t idle_now,
-                           uint32_t t, const Task& T, uint32_t m0, uint32_t m1) {
+                           uint32_t t, const Task& T, uint32_t m0, uint32_t m1, int tail_level) {
   // Ranges are split down to two elements near the root (where every element
   // heads a large subtree) and only from 64 elements further down.
   const int n = (int)p.plan->n;
@@ -218,6 +218,7 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
     const uint32_t cnt = lv[L].cnt, ce = lv[L].cur_e;
     if (ce >= cnt) continue;
     if (cnt - ce >= 2) { Ls = L; mode = 1; break; }
+    if (L == tail_level) continue;  // the tail stage takes whole entries only
     const uint32_t min_split = (L + 5 <= n) ? 2u : (p.split_deep ? p.split_deep : 64u);
     if (lv[L].dn[ce] - lv[L].cur_k >= min_split) { Ls = L; mode = 2; break; }
   }
@@ -289,6 +290,181 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
   return k;
 }
 
+// ---------------------------------------------------------------- tail stage
+
+constexpr unsigned long long kTailSat = 1ULL << 58;  // a warp's sum of 32 saturated counts stays below 2^63
+
+__device__ __forceinline__ unsigned long long sat_mul(unsigned long long a, unsigned long long b) {
+  if (a == 0 || b == 0) return 0;
+  return a > kTailSat / b ? kTailSat : min(kTailSat, a * b);
+}
+
+// Injective assignments of a label group of g <= kTailGroup tail positions,
+// from N[M]: the number of candidates whose set of group members they are a
+// candidate of is exactly M.  Members served by candidates of one class M
+// form a subset R of M, in N[M] (N[M] - 1) ... (N[M] - |R| + 1) ways; a
+// dynamic program over the set of served members.  Without injectivity
+// (homo) it is the product of the members' candidate counts.  Saturates.
+__device__ __noinline__ unsigned long long group_assignments(uint32_t g, const unsigned long long* N, int homo) {
+  const uint32_t full = (1u << g) - 1u;
+  if (homo) {
+    unsigned long long prod = 1;
+    for (uint32_t i = 0; i < g; i++) {
+      unsigned long long c = 0;
+      for (uint32_t M = 1; M <= full; M++)
+        if ((M >> i) & 1u) c = min(kTailSat, c + N[M]);
+      prod = sat_mul(prod, c);
+    }
+    return prod;
+  }
+  unsigned long long f[1u << kTailGroup], h[1u << kTailGroup];
+  for (uint32_t S = 0; S <= full; S++) f[S] = S == 0 ? 1ull : 0ull;
+  for (uint32_t M = 1; M <= full; M++) {
+    if (!N[M]) continue;
+    for (uint32_t S = 0; S <= full; S++) h[S] = 0;
+    for (uint32_t S = 0; S <= full; S++) {
+      if (!f[S]) continue;
+      const uint32_t fr = M & ~S;
+      for (uint32_t R = fr;; R = (R - 1u) & fr) {  // every subset of fr, the empty one last
+        unsigned long long ways = 1;
+        for (uint32_t r = 0, k = (uint32_t)__popc(R); r < k; r++) ways = sat_mul(ways, N[M] > r ? N[M] - r : 0ull);
+        if (ways) h[S | R] = min(kTailSat, h[S | R] + sat_mul(f[S], ways));
+        if (R == 0) break;
+      }
+    }
+    for (uint32_t S = 0; S <= full; S++) f[S] = h[S];
+  }
+  return f[full];
+}
+
+// Prefix m[0 .. L] of entry e of level L.
+__device__ __forceinline__ void load_prefix(uint32_t* m, const LevelSM* lv, int L, uint32_t e, uint32_t m0,
+                                            uint32_t m1) {
+  m[0] = m0; m[1] = m1;
+  uint32_t idx = e;
+  for (int l2 = L; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
+}
+
+// Counts the completions of the entries of level L (= the anchor's tail_at:
+// complete matches of the positions before the independent tail).  For each
+// label group of the tail, every member's candidates are listed from its
+// driver segment (32 (entry, element) pairs at a time, as in run_levels) and
+// classified by the other members they are candidates of; a candidate is
+// counted under the first member it belongs to, in per-entry class counters
+// kept in the unused levels above L.  Each entry's completions are the
+// product over groups of group_assignments.  A group is not looked at for
+// entries whose product is already 0.  Returns false when the update was
+// stopped (cap, deadline or stop flag).
+__device__ __noinline__ bool tail_stage(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int L,
+                                        uint32_t lane, const Task& T, const PlanAnchor* A, uint32_t m0,
+                                        uint32_t m1, TaskAcc& acc) {
+  const uint32_t t = T.upd;
+  volatile unsigned int* stop = p.stop;
+  LevelSM& S = lv[L];
+  const uint32_t ce = S.cur_e, cnt = S.cnt, ck = S.cur_k;
+  const uint32_t ne = cnt > ce ? cnt - ce : 0u;
+  const bool has = lane < ne;
+  const uint32_t e_mine = ce + (has ? lane : 0u);
+  uint32_t* cntr = reinterpret_cast<uint32_t*>(&lv[L + 1]);  // [class][entry], levels L+1.. are unused here
+  const uint32_t pmask = A->prefix_mask;
+  uint32_t m[kMaxQ];
+  unsigned long long prod = has ? 1ull : 0ull, bytes = 0;
+  bool stopped = false;
+  uint32_t gp = 0, it = 0;
+  for (uint32_t gi = 0; gi < A->n_groups; gi++) {
+    const uint32_t g = A->gsize[gi];
+    const uint32_t ncls = (1u << g) - 1u;
+    for (uint32_t c = 0; c < ncls; c++) cntr[c * 32 + lane] = 0;
+    __syncwarp();
+    for (uint32_t j = 0; j < g && !stopped; j++) {
+      const uint32_t ps = A->gpos[gp + j];
+      uint32_t dlo = 0, dn = 0, dsel = 0;
+      if (prod) {
+        if (ps == (uint32_t)L + 1) {  // the entry's own driver, found when it was pushed
+          const uint32_t skip = lane == 0 ? ck : 0u;
+          dlo = S.dlo[e_mine] + skip; dn = S.dn[e_mine] - skip; dsel = S.dsel[e_mine];
+        } else {
+          load_prefix(m, lv, L, e_mine, m0, m1);
+          unsigned long long b4 = 0;
+          if (!pick_driver(p, A, ps, m, (int32_t)t, dlo, dn, dsel, b4)) dn = 0;
+          bytes += b4;
+        }
+      }
+      const uint32_t incl = warp_incl_scan(dn, lane);
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      for (uint32_t base = 0; base < total; base += 32) {
+        if ((++it & 63) == 0) {
+          unsigned int st = 0;
+          if (lane == 0) {
+            if (p.deadline_ns && global_ns() - p.sstat->launch_t0 > p.deadline_ns)
+              atomicCAS(const_cast<unsigned int*>(stop) + t, 0u, kStopDeadline);
+            st = stop[t];
+          }
+          if (__shfl_sync(0xffffffffu, st, 0)) { stopped = true; break; }
+        }
+        acc.iters++;
+        const uint32_t gidx = base + lane;
+        uint32_t owner = 0;
+#pragma unroll
+        for (uint32_t step = 16; step; step >>= 1) {
+          const uint32_t v = __shfl_sync(0xffffffffu, incl, owner + step - 1);
+          if (v <= gidx) owner += step;
+        }
+        const uint32_t own = owner & 31u;
+        const uint32_t prev = __shfl_sync(0xffffffffu, incl, (owner - 1u) & 31u);
+        const uint32_t o_dlo = __shfl_sync(0xffffffffu, dlo, own);
+        const uint32_t o_dsel = __shfl_sync(0xffffffffu, dsel, own);
+        if (gidx < total) {
+          const uint32_t kk = gidx - (owner ? prev : 0u);
+          const uint32_t x = pool[(uint64_t)o_dlo + kk];
+          load_prefix(m, lv, L, ce + owner, m0, m1);
+          if (check_candidate(p, pool, A, ps, x, m, o_dsel, (int32_t)t, pmask)) {
+            uint32_t M = 1u << j;
+            bool seen = false;
+            for (uint32_t i = 0; i < g && !seen; i++) {
+              if (i == j || !check_candidate(p, pool, A, A->gpos[gp + i], x, m, 0xffu, (int32_t)t, pmask)) continue;
+              if (i < j) seen = true;
+              else M |= 1u << i;
+            }
+            if (!seen) atomicAdd(&cntr[(M - 1u) * 32u + owner], 1u);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    gp += g;
+    if (stopped) break;
+    if (prod) {
+      unsigned long long N[1u << kTailGroup];
+      N[0] = 0;
+      for (uint32_t c = 1; c <= ncls; c++) N[c] = cntr[(c - 1u) * 32u + lane];
+      prod = sat_mul(prod, group_assignments(g, N, p.homo));
+    }
+    __syncwarp();
+    if (!__any_sync(0xffffffffu, prod != 0)) break;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+  acc.bytes += bytes;
+  if (stopped) return false;
+  unsigned long long sum = prod;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) S.cur_e = cnt;
+  __syncwarp();
+  acc.cnt += sum;
+  if (sum && p.cap) {
+    unsigned int hit = 0;
+    if (lane == 0) {
+      const unsigned long long old = atomicAdd(&p.count[t], acc.cnt);
+      acc.cnt = 0;
+      if (old + sum >= p.cap) { stop[t] = kStopCap; hit = 1; }
+    }
+    if (__shfl_sync(0xffffffffu, hit, 0)) return false;
+  }
+  return true;
+}
+
 // Depth-first walk over chunked levels starting at level `d` (see the file
 // comment); positions 0 and 1 hold m0 and m1.  EN compiles the match-set
 // append in: it is a separate instantiation so that the counting-only kernel
@@ -301,6 +477,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
   volatile unsigned int* stop = p.stop;
   uint32_t iter = 0;
   const unsigned long long t_start = global_ns();
+  const int tail_level = (!EN && p.tail && A->tail_at) ? (int)A->tail_at : -1;
   while (d >= 1) {
     ++iter;
     if ((iter & 63) == 0 && p.deadline_ns) {
@@ -339,7 +516,12 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       idle_now = __shfl_sync(0xffffffffu, idle_now, 0);
       acc.checks++;
       if (idle_now) acc.checks_hungry++;
-      if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1);
+      if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1, tail_level);
+    }
+    if (d == tail_level) {
+      if (!tail_stage(p, pool, lv, d, lane, T, A, m0, m1, acc)) break;
+      d--;
+      continue;
     }
     LevelSM& L = lv[d];
     const uint32_t cnt = L.cnt, ce = L.cur_e, ck = L.cur_k;
@@ -581,7 +763,7 @@ __global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint3
 }
 
 template <int W, bool EN>
-__global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
+__global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search(SearchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint4 task_scratch[W * 10];  // one 160-byte record per warp
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -40,7 +40,7 @@ class Engine:
                  deadline_ns: int = 0, hbm_budget_bytes: int = 0, warps_per_block: int = 0,
                  blocks_per_sm: int = 0, turboflux_compat: bool = False, vertex_headroom: int = 0,
                  graphs: bool = False, shard_rank: int = 0, shard_count: int = 1, donate_every: int = 0,
-                 split_deep: int = 0, enum_capacity: int = 0):
+                 split_deep: int = 0, enum_capacity: int = 0, tail_enumerate: bool = False):
         self.lib = load_library()
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -63,6 +63,7 @@ class Engine:
         cfg.donate_every = int(donate_every)
         cfg.split_deep = int(split_deep)
         cfg.enum_capacity = int(enum_capacity)
+        cfg.tail_enumerate = int(bool(tail_enumerate))
         self.cfg = cfg
         h = C.c_void_p()
         check(self.lib, self.lib.csm_gpu_create(C.byref(cfg), C.byref(h)))
@@ -94,7 +95,7 @@ class Engine:
 
     def attach(self, vlabels, edges, algorithm: str | int = "parallel_graphflow", *, max_results: int = 0,
                want_hash: bool = False, warps_per_block: int = 0, blocks_per_sm: int = 0,
-               enum_capacity: int = 0) -> "Engine":
+               enum_capacity: int = 0, tail_enumerate: bool = False) -> "Engine":
         """A standing query on this engine's graph; its results follow every submit to this engine."""
         cfg = CsmCfg()
         self.lib.csm_gpu_default_cfg(C.byref(cfg))
@@ -104,6 +105,7 @@ class Engine:
         cfg.warps_per_block = int(warps_per_block)
         cfg.blocks_per_sm = int(blocks_per_sm)
         cfg.enum_capacity = int(enum_capacity)
+        cfg.tail_enumerate = int(bool(tail_enumerate))
         vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
         e = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 3)
         h = C.c_void_p()

@@ -172,3 +172,40 @@ def test_oracle_initial_count_matches_the_reference_csm(case):
     want = json.loads((g["dir"] / "initial.json").read_text())
     got = pyoracle.initial_count(g["qv"], g["qe"], g["vl"], g["e"], homo=g["params"]["homo"])
     assert got == want["graphflow"] == want["symbi"] == want["turboflux"]
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_oracle_tail_counting_gives_the_enumeration_counts(case):
+    """The counting search (want_hash = 0: the independent tail of each order is
+    counted, not enumerated) gives the reference's counts."""
+    g = load_golden(case)
+    cap = g["params"]["max_results"] or 0
+    kw = dict(max_results=cap, homo=g["params"]["homo"])
+    full = pyoracle.run(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], want_hash=True, **kw)
+    tail = pyoracle.run(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], want_hash=False, **kw)
+    assert np.array_equal(tail["pos"], full["pos"]) and np.array_equal(tail["neg"], full["neg"])
+    assert np.array_equal(tail["status"], full["status"])
+    assert np.array_equal(tail["pos"], g["exp"]["symbi_pos"])
+
+
+# sparse queries over three labels whose orders end in tails with three
+# vertices of one label; the second one has capped updates
+GROUP3 = [
+    (["--avg-degree", "3", "--seed", "3", "--query", "10:sparse:1"], 0),
+    (["--avg-degree", "4", "--seed", "1", "--query", "9:sparse:0"], 1_000_000),
+]
+
+
+@pytest.mark.parametrize("spec", range(len(GROUP3)))
+def test_oracle_tail_counting_with_groups_of_three(gen_dir, spec):
+    from paracosm_b200 import workload
+    args, cap = GROUP3[spec]
+    w = workload.generate("c2", gen_dir / f"tail3_{spec}", extra=[
+        "--log2-n", "11", "--vlabels", "3", "--zipf", "0", "--elabels", "2", "--updates", "300",
+        "--insert-frac", "0.8"] + args)
+    qv, qe = w.queries[0]
+    full = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream, max_results=cap, want_hash=True)
+    tail = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream, max_results=cap, want_hash=False)
+    assert np.array_equal(tail["pos"], full["pos"]) and np.array_equal(tail["neg"], full["neg"])
+    assert np.array_equal(tail["status"], full["status"])
+    assert full["pos"].sum() > 0
