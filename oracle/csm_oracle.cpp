@@ -288,10 +288,23 @@ struct Searcher {
   // each group, every member's candidates are listed (adding its bytes) and
   // classified by membership in the group's other members; an element is
   // counted once, under the first member it is a candidate of.  A group is
-  // only looked at while the product is nonzero.
+  // only looked at while the product is nonzero.  As in the engine, a prefix
+  // whose first tail position has an empty back-neighbour segment stops
+  // there (the engine drops it before the tail is looked at).
   void count_tail(uint32_t oi, uint32_t first) {
     const uint64_t kSat = 1ULL << 58;
     const auto& o = order[oi];
+    {
+      const uint32_t u = o[first];
+      bool empty = false;
+      uint64_t b = 0;
+      for (size_t i = 0; i < q.nbr[u].size(); i++) {
+        const uint32_t sz = g.seg_size(m[q.nbr[u][i]], q.vlabel[u], q.elab[u][i]);
+        b += 4ULL * sz;
+        if (sz == 0) empty = true;
+      }
+      if (empty) { bytes += b; return; }
+    }
     std::vector<char> done(q.n, 0);
     uint64_t prod = 1;
     std::vector<uint32_t> c;

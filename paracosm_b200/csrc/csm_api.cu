@@ -437,7 +437,10 @@ static void search_shape(const csm_ctx* q, uint32_t& warps, uint32_t& bps) {
   warps = q->cfg.warps_per_block ? q->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   bps = q->cfg.blocks_per_sm ? q->cfg.blocks_per_sm : 0;
-  if (!bps) bps = std::max<uint32_t>(1, search_max_blocks(q->nq, warps, q->d_enum != nullptr));
+  if (!bps) {
+    const int mode = q->d_enum ? 1 : ((!q->cfg.want_hash && !q->cfg.tail_enumerate) ? 2 : 0);
+    bps = std::max<uint32_t>(1, search_max_blocks(q->nq, warps, mode));
+  }
 }
 
 // One standing query q over the owner o's union graph: index to the union
@@ -950,15 +953,16 @@ static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_
   // the default shape (8 warps, every resident block), then the others; a
   // shape replaces the default only when it is at least 5 % faster, since
   // capped updates make single timings vary by a few percent
-  uint32_t best_w = 8, best_b = std::max<uint32_t>(1, search_max_blocks(ctx->nq, 8));
+  const int kmode = ctx->d_enum ? 1 : ((!ctx->cfg.want_hash && !ctx->cfg.tail_enumerate) ? 2 : 0);  // as the batches run
+  uint32_t best_w = 8, best_b = std::max<uint32_t>(1, search_max_blocks(ctx->nq, 8, kmode));
   float best = 0;
   rc = tune_run(ctx, B, best_w, best_b, &best);
   if (rc) return rc;
   const float def_ms = best;
   for (uint32_t w : {4u, 8u, 16u}) {
-    const uint32_t bmax = search_max_blocks(ctx->nq, w);  // resident blocks per SM
+    const uint32_t bmax = search_max_blocks(ctx->nq, w, kmode);  // resident blocks per SM
     for (uint32_t b = std::max<uint32_t>(1, bmax > 3 ? bmax - 3 : 1); b <= bmax; b++) {
-      if (w == 8 && b == std::max<uint32_t>(1, search_max_blocks(ctx->nq, 8))) continue;
+      if (w == 8 && b == std::max<uint32_t>(1, search_max_blocks(ctx->nq, 8, kmode))) continue;
       rc = tune_run(ctx, B, w, b, &ms);
       if (rc) return rc;
       if (ms < best && ms < 0.95f * def_ms) { best = ms; best_w = w; best_b = b; }

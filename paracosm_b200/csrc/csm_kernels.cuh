@@ -148,7 +148,7 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
                        uint32_t* safe, unsigned int* error, uint32_t shard_rank = 0, uint32_t shard_count = 1,
                        uint32_t turboflux_compat = 0, uint32_t dup_zero = 0);
 size_t search_smem_bytes(uint32_t n_q, uint32_t warps);
-uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, bool with_enum = false);
+uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, int mode = 0);  // mode: 0 plain, 1 match sets, 2 tail counting
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s);
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,

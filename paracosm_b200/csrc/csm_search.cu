@@ -355,7 +355,7 @@ __device__ __forceinline__ void load_prefix(uint32_t* m, const LevelSM* lv, int 
 // product over groups of group_assignments.  A group is not looked at for
 // entries whose product is already 0.  Returns false when the update was
 // stopped (cap, deadline or stop flag).
-__device__ __noinline__ bool tail_stage(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int L,
+__device__ __forceinline__ bool tail_stage(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int L,
                                         uint32_t lane, const Task& T, const PlanAnchor* A, uint32_t m0,
                                         uint32_t m1, TaskAcc& acc) {
   const uint32_t t = T.upd;
@@ -466,10 +466,11 @@ __device__ __noinline__ bool tail_stage(const SearchParams& p, const uint32_t* p
 }
 
 // Depth-first walk over chunked levels starting at level `d` (see the file
-// comment); positions 0 and 1 hold m0 and m1.  EN compiles the match-set
-// append in: it is a separate instantiation so that the counting-only kernel
-// keeps its register budget.
-template <bool EN>
+// comment); positions 0 and 1 hold m0 and m1.  MODE 1 compiles the
+// match-set append in, MODE 2 the tail stage; each is a separate
+// instantiation so that the plain counting kernel (MODE 0) keeps its
+// register budget.
+template <int MODE>
 __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM* lv, int d, uint32_t lane,
                            const Task& T, const PlanAnchor* A, uint32_t m0, uint32_t m1, TaskAcc& acc) {
   const uint32_t n = p.plan->n;
@@ -477,7 +478,8 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
   volatile unsigned int* stop = p.stop;
   uint32_t iter = 0;
   const unsigned long long t_start = global_ns();
-  const int tail_level = (!EN && p.tail && A->tail_at) ? (int)A->tail_at : -1;
+  constexpr bool EN = MODE == 1;
+  const int tail_level = (MODE == 2 && p.tail && A->tail_at) ? (int)A->tail_at : -1;
   while (d >= 1) {
     ++iter;
     if ((iter & 63) == 0 && p.deadline_ns) {
@@ -518,10 +520,12 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       if (idle_now) acc.checks_hungry++;
       if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1, tail_level);
     }
-    if (d == tail_level) {
-      if (!tail_stage(p, pool, lv, d, lane, T, A, m0, m1, acc)) break;
-      d--;
-      continue;
+    if constexpr (MODE == 2) {
+      if (d == tail_level) {
+        if (!tail_stage(p, pool, lv, d, lane, T, A, m0, m1, acc)) break;
+        d--;
+        continue;
+      }
     }
     LevelSM& L = lv[d];
     const uint32_t cnt = L.cnt, ce = L.cur_e, ck = L.cur_k;
@@ -647,7 +651,7 @@ __device__ __forceinline__ void flush_acc(const SearchParams& p, uint32_t t, uin
 
 // Root task: positions 0 and 1 are the updated edge; level 1 holds the driver
 // segment of position 2.
-template <bool EN>
+template <int MODE>
 __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, const Task& T,
                          TaskAcc& acc) {
   const uint32_t n = p.plan->n;
@@ -659,7 +663,7 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
     if (lane == 0) {
       acc.cnt += 1;
       if (p.want_hash) acc.hash += mix64(pair_hash(A->pos[0].qv, m0) + pair_hash(A->pos[1].qv, m1));
-      if (EN) {
+      if (MODE == 1) {
         const unsigned long long r = atomicAdd(p.enum_n, 1ull);
         if (r < p.enum_cap) {
           uint32_t* rec = p.enum_buf + r * p.enum_stride;
@@ -701,13 +705,13 @@ __device__ void run_root(const SearchParams& p, const uint32_t* pool, LevelSM* l
     lv[1].dlo[0] = dlo0; lv[1].dn[0] = minsz; lv[1].dsel[0] = (uint8_t)sel;
   }
   __syncwarp();
-  run_levels<EN>(p, pool, lv, 1, lane, T, A, m0, m1, acc);
+  run_levels<MODE>(p, pool, lv, 1, lane, T, A, m0, m1, acc);
 }
 
 // Donated task: rebuild the chain of the partial match (exhausted levels
 // 1 .. depth-1) and continue from level `depth`.  `hw` holds record words
 // 0..4 in lanes 0..4 and `mv` holds m[lane] (see DTask).
-template <bool EN>
+template <int MODE>
 __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM* lv, uint32_t lane, uint32_t hw,
                             uint32_t mv, TaskAcc& acc, uint32_t& upd_out, unsigned long long ticket,
                             unsigned long long seen_seq) {
@@ -749,7 +753,7 @@ __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM
   const unsigned int stopped =
       __shfl_sync(0xffffffffu, lane == 0 ? *(volatile unsigned int*)(p.stop + upd) : 0u, 0);
   if (stopped) return;
-  run_levels<EN>(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
+  run_levels<MODE>(p, pool, lv, (int)depth, lane, T, A, m0, m1, acc);
 }
 
 // Per launch: tickets keep counting up across launches (the ring's slot
@@ -762,8 +766,10 @@ __global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint3
   ss->launch_t0 = global_ns();
 }
 
-template <int W, bool EN>
-__global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search(SearchParams p) {
+// Kernel body; MODE 0 counts (and hashes), 1 also appends match sets, 2
+// counts independent tails (tail_stage).
+template <int W, int MODE>
+__device__ __forceinline__ void search_body(const SearchParams& p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint4 task_scratch[W * 10];  // one 160-byte record per warp
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -789,7 +795,7 @@ __global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search
       atomicCAS(const_cast<unsigned int*>(stop) + T.upd, 0u, kStopDeadline);
     // stop flags change under our feet: one lane reads, the warp follows it
     const unsigned int stopped = __shfl_sync(0xffffffffu, lane == 0 ? stop[T.upd] : 0u, 0);
-    if (!stopped) run_root<EN>(p, pool, lv, lane, T, acc);
+    if (!stopped) run_root<MODE>(p, pool, lv, lane, T, acc);
     const unsigned long long te = global_ns();
     busy_ns += te - tb;
     root_ns += te - tb;
@@ -860,7 +866,7 @@ __global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search
     __syncwarp();
     uint32_t t = 0;
     const unsigned long long tb = global_ns();
-    run_donated<EN>(p, pool, lv, lane, hw, mv, acc, t, claimed, seen);
+    run_donated<MODE>(p, pool, lv, lane, hw, mv, acc, t, claimed, seen);
     busy_ns += global_ns() - tb;
     max_task = max(max_task, global_ns() - tb);
     if (t < p.batch) flush_acc(p, t, lane, acc);
@@ -878,46 +884,78 @@ __global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search
 
 // Blocks of the search kernel that can be resident on one SM for this query
 // size (registers, shared memory and warp slots), from the occupancy API.
-namespace {
-
 template <int W, bool EN>
-cudaError_t search_occupancy(int* nb, size_t smem) {
-  cudaFuncSetAttribute(k_search<W, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_search<W, EN>, W * 32, smem);
+__global__ void __launch_bounds__(W * 32) k_search(SearchParams p) {
+  search_body<W, EN ? 1 : 0>(p);
 }
 
-template <int W, bool EN>
-void search_launch(const SearchParams& p, uint32_t blocks, size_t smem, cudaStream_t s) {
-  cudaFuncSetAttribute(k_search<W, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_search<W, EN><<<blocks, W * 32, smem, s>>>(p);
+// The tail-counting variant keeps the plain kernel's resident blocks (three
+// of 8 warps, two of 16) under a register bound.
+template <int W>
+__global__ void __launch_bounds__(W * 32, W == 16 ? 2 : 768 / (W * 32)) k_search_tail(SearchParams p) {
+  search_body<W, 2>(p);
+}
+
+namespace {
+
+// mode: 0 plain, 1 match sets, 2 tail counting
+template <int W>
+cudaError_t search_occupancy(int* nb, size_t smem, int mode) {
+  if (mode == 2) {
+    cudaFuncSetAttribute(k_search_tail<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_search_tail<W>, W * 32, smem);
+  }
+  if (mode == 1) {
+    cudaFuncSetAttribute(k_search<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_search<W, true>, W * 32, smem);
+  }
+  cudaFuncSetAttribute(k_search<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_search<W, false>, W * 32, smem);
+}
+
+template <int W>
+void search_launch(const SearchParams& p, uint32_t blocks, size_t smem, cudaStream_t s, int mode) {
+  if (mode == 2) {
+    cudaFuncSetAttribute(k_search_tail<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_search_tail<W><<<blocks, W * 32, smem, s>>>(p);
+  } else if (mode == 1) {
+    cudaFuncSetAttribute(k_search<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_search<W, true><<<blocks, W * 32, smem, s>>>(p);
+  } else {
+    cudaFuncSetAttribute(k_search<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_search<W, false><<<blocks, W * 32, smem, s>>>(p);
+  }
 }
 
 }  // namespace
 
 // Blocks of the search kernel that can be resident on one SM for this query
 // size (registers, shared memory and warp slots), from the occupancy API.
-// `with_enum` selects the instantiation that appends match sets.
-uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, bool with_enum) {
+// `mode` selects the instantiation: 0 plain counting (and hashes), 1 match
+// sets, 2 tail counting.
+uint32_t search_max_blocks(uint32_t n_q, uint32_t warps, int mode) {
   const size_t smem = search_smem_bytes(n_q, warps);
   int nb = 0;
   cudaError_t e = cudaSuccess;
   switch (warps) {
-    case 4: e = with_enum ? search_occupancy<4, true>(&nb, smem) : search_occupancy<4, false>(&nb, smem); break;
-    case 16: e = with_enum ? search_occupancy<16, true>(&nb, smem) : search_occupancy<16, false>(&nb, smem); break;
-    default: e = with_enum ? search_occupancy<8, true>(&nb, smem) : search_occupancy<8, false>(&nb, smem); break;
+    case 4: e = search_occupancy<4>(&nb, smem, mode); break;
+    case 16: e = search_occupancy<16>(&nb, smem, mode); break;
+    default: e = search_occupancy<8>(&nb, smem, mode); break;
   }
   if (e != cudaSuccess) { cudaGetLastError(); return 0; }
   return (uint32_t)nb;
 }
 
+int search_mode(const SearchParams& p) { return p.enum_buf ? 1 : (p.tail ? 2 : 0); }
+
 void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_t warps, cudaStream_t s) {
   const size_t smem = search_smem_bytes(n_q, warps);
   if (p.q) k_search_prep<<<1, 1, 0, s>>>(p.q, p.n_tasks, p.task_cap, p.sstat, p.error);
-  const bool en = p.enum_buf != nullptr;
+  const int mode = search_mode(p);
   switch (warps) {
-    case 4: en ? search_launch<4, true>(p, blocks, smem, s) : search_launch<4, false>(p, blocks, smem, s); break;
-    case 16: en ? search_launch<16, true>(p, blocks, smem, s) : search_launch<16, false>(p, blocks, smem, s); break;
-    default: en ? search_launch<8, true>(p, blocks, smem, s) : search_launch<8, false>(p, blocks, smem, s); break;
+    case 4: search_launch<4>(p, blocks, smem, s, mode); break;
+    case 16: search_launch<16>(p, blocks, smem, s, mode); break;
+    default: search_launch<8>(p, blocks, smem, s, mode); break;
   }
 }
 

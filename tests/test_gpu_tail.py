@@ -76,7 +76,8 @@ def test_tail_counts_equal_the_oracle(case, algo, mode):
     _check_counts(res, want, cap, _dups(g["e"], g["stream"]) if algo == "parallel_calig" else None)
     # the reference's own counts (golden) agree too
     assert np.array_equal(want["neg"], g["exp"]["symbi_neg"])
-    assert init == pyoracle.initial_count(g["qv"], g["qe"], g["vl"], g["e"], homo=homo)
+    # InitialMatching on the graph after the stream
+    assert init == pyoracle.initial_count(g["qv"], g["qe"], g["vl"], g["e"], g["stream"], homo=homo)
 
 
 @pytest.mark.parametrize("algo", ["parallel_graphflow", "parallel_symbi"])
