@@ -38,7 +38,7 @@ METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact cou
 # DRAM bytes (read + write) of one k_search launch over a 4,096-update C3
 # batch, from the ncu capture summarised in profiles/k_search_c3_b4096.md;
 # scaled to a launch by the updates it processes.
-SEARCH_DRAM_BYTES_PER_4096 = 98.4e6
+SEARCH_DRAM_BYTES_PER_4096 = 93.0e6
 
 CONFIGS = {
     "c3": {
