@@ -61,6 +61,9 @@ extern "C" {
 #define CSM_ALGO_SYMBI 2     /* -a parallel_symbi / symbi: DCS over a DAG of all query edges */
 #define CSM_ALGO_CALIG 3     /* -a parallel_calig / calig: CaLiG-style lighting filter over every query edge;
                                 an insertion of a present edge counts 0 (Parallel_CaLiG/parallel_calig.cpp:1233) */
+#define CSM_ALGO_NEWSP 4     /* -a parallel_newsp / newsp: NewSP-style neighbour-label-frequency filter
+                                (Parallel_NewSP/matching/CSMPP.cpp:81-113 indexCheck); leaf vertices counted
+                                together when only counts are wanted (its isolated vertices, :641) */
 
 /* ---- execution modes ------------------------------------------------ */
 #define CSM_MODE_BATCHED 0   /* many updates per launch sequence (default) */

@@ -23,7 +23,7 @@ CSM_EDEVICE = -7
 
 ST_OK, ST_CAPPED, ST_TIMED_OUT, ST_INVALID = 0, 1, 2, 3
 
-ALGO_GRAPHFLOW, ALGO_TURBOFLUX, ALGO_SYMBI, ALGO_CALIG = 0, 1, 2, 3
+ALGO_GRAPHFLOW, ALGO_TURBOFLUX, ALGO_SYMBI, ALGO_CALIG, ALGO_NEWSP = 0, 1, 2, 3, 4
 MODE_BATCHED, MODE_PLAIN = 0, 1
 
 # The reference's -a names (ParaCOSM/CSM/matching/main.cpp:740-757) and the engine algorithm behind each.
@@ -37,6 +37,9 @@ ALGORITHMS = {
     # CaLiG is its own program in the reference (ParaCOSM/CSM/matching/Parallel_CaLiG)
     "calig": ALGO_CALIG,
     "parallel_calig": ALGO_CALIG,
+    # NewSP has its own driver in the reference (ParaCOSM/CSM/matching/Parallel_NewSP/matching/main.cpp)
+    "newsp": ALGO_NEWSP,
+    "parallel_newsp": ALGO_NEWSP,
 }
 
 UPDATE_DTYPE = np.dtype(

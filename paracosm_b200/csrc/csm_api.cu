@@ -1136,7 +1136,7 @@ const char* csm_gpu_strerror(int code) {
 
 int csm_gpu_create(const csm_cfg* cfg, csm_ctx** out) {
   if (!cfg || !out) return set_err(CSM_EINVAL, "null argument");
-  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_CALIG)
+  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_NEWSP)
     return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   if (cfg->max_batch > kMaxBatch) return set_err(CSM_EINVAL, "max_batch above %u", kMaxBatch);
   if (cfg->shard_count > 1 && cfg->shard_rank >= cfg->shard_count)
@@ -1262,7 +1262,7 @@ int csm_gpu_attach_query(csm_ctx* owner, const csm_cfg* cfg, uint32_t n_qv, cons
   if (!owner || !cfg || !out || !q_vlabels || (n_qe && !q_edges)) return set_err(CSM_EINVAL, "null argument");
   if (owner->owner) return set_err(CSM_ESTATE, "attach to the context that owns the graph");
   if (!owner->has_graph || !owner->has_plan) return set_err(CSM_ESTATE, "the owner needs a graph and a built index");
-  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_CALIG)
+  if (cfg->algorithm < 0 || cfg->algorithm > CSM_ALGO_NEWSP)
     return set_err(CSM_EINVAL, "unknown algorithm %d", cfg->algorithm);
   CK(cudaSetDevice(owner->dev));
   CK(cudaStreamSynchronize(owner->st));

@@ -458,7 +458,7 @@ static int index_finish(IndexState& ix, DevMem& mem, const DevGraph& g, const In
       D.n_edges++;
     }
   }
-  if (algo == CSM_ALGO_CALIG) {
+  if (algo == CSM_ALGO_CALIG || algo == CSM_ALGO_NEWSP) {
     // d1 requirements: per (vertex label, edge label) pair of u's query
     // edges, as many neighbours as u has of that pair (one under homo)
     D.lighting = 1;
@@ -508,7 +508,9 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   index_free(ix, mem);
   ix.algo = algo;
   ix.sm_count = sm_count > 0 ? sm_count : 148;
-  if (algo != CSM_ALGO_TURBOFLUX && algo != CSM_ALGO_SYMBI && algo != CSM_ALGO_CALIG) return CSM_OK;
+  if (algo != CSM_ALGO_TURBOFLUX && algo != CSM_ALGO_SYMBI && algo != CSM_ALGO_CALIG && algo != CSM_ALGO_NEWSP)
+    return CSM_OK;
+  const bool lighting = algo == CSM_ALGO_CALIG || algo == CSM_ALGO_NEWSP;
   const uint32_t nq = q.n;
   const auto& ql = *q.vlabels;
   const auto& nbr = *q.nbr;
@@ -521,12 +523,12 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
       if (u < nbr[u][i]) { edges.emplace_back(u, nbr[u][i]); e_lab.push_back(el[u][i]); }
   const uint32_t ne = (uint32_t)edges.size();
   if (ne == 0 || ne > kMaxQE || nq > kMaxQ) return set_err(CSM_EUNSUPPORTED, "query size outside the index limits");
-  if (algo == CSM_ALGO_CALIG && 2 * ne > kMaxQE)
+  if (lighting && 2 * ne > kMaxQE)
     return set_err(CSM_EUNSUPPORTED, "query has more than %u edges (lighting filter limit)", kMaxQE / 2);
   std::vector<std::vector<uint32_t>> par(nq), chd(nq), par_l(nq), chd_l(nq);
   std::vector<uint32_t> order;
   uint32_t root = 0;
-  if (algo == CSM_ALGO_CALIG) {
+  if (lighting) {
     // lighting: every query neighbour is a child, nobody has a parent
     for (uint32_t u = 0; u < nq; u++) {
       order.push_back(u);
@@ -538,7 +540,11 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
     if (rc) return rc;
   }
   if (order.size() != nq) return set_err(CSM_EINVAL, "query graph is not connected");
-  return index_finish(ix, mem, g, q, algo, root, order, par, chd, par_l, chd_l, st, launches);
+  const int rc = index_finish(ix, mem, g, q, algo, root, order, par, chd, par_l, chd_l, st, launches);
+  // the NewSP-style plugin filters candidates by the neighbour-label
+  // frequencies alone (d1); d2 is still kept
+  if (rc == CSM_OK && algo == CSM_ALGO_NEWSP) ix.d2 = ix.bits.d1;
+  return rc;
 }
 
 int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,

@@ -17,14 +17,18 @@
 // CSR) of vertices whose flag changed at a DAG neighbour, level by level in
 // DAG order.
 //
-// The CaLiG-style plugin uses the same machinery for its lighting filter
-// (ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:337-429): the
-// "DAG" has no parents and makes every query neighbour a child, d1 is the
-// label test plus, per (vertex label, edge label) pair of u's query edges, at
-// least as many neighbours of that pair as u has (CaLiG's distinct witnesses
-// for same-label neighbours, counted), and d2 is d1 with every query
-// neighbour supported by a d1 neighbour.  Both levels are functions of the
-// graph, monotone in its edges, and contain the reference's lighting.
+// The CaLiG-style and NewSP-style plugins use the same machinery for their
+// filters, in a "lighting" mode: the DAG has no parents and makes every
+// query neighbour a child; d1 is the label test plus, per (vertex label, edge
+// label) pair of u's query edges, at least as many neighbours of that pair as
+// u has; d2 is d1 with every query neighbour supported by a d1 neighbour.
+// Both levels are functions of the graph and monotone in its edges.  d2
+// contains CaLiG's lighting (ParaCOSM/CSM/matching/Parallel_CaLiG/
+// parallel_calig.cpp:337-429: distinct lit witnesses for every query
+// neighbour) and is that plugin's filter.  d1 implies NewSP's index check
+// (ParaCOSM/CSM/matching/Parallel_NewSP/matching/CSMPP.cpp:81-113: at
+// least as many neighbours of each vertex label and of each edge label) and
+// is that plugin's filter.
 //
 // Every batch first brings the flags to the batch's union graph
 // (a superset of the graph any of its updates sees, and the flags are

@@ -394,6 +394,12 @@ class Parallel_CaLiG(_ParallelMixin, matching):
     ALGO = "parallel_calig"
 
 
+class CSMPP(_ParallelMixin, matching):
+    """NewSP's plugin class (ParaCOSM/CSM/matching/Parallel_NewSP/matching/CSMPP.h:8-183): neighbour-label-frequency
+    filter; leaf vertices counted together when only counts are wanted."""
+    ALGO = "parallel_newsp"
+
+
 PLUGINS = {
     "graphflow": Graphflow,
     "turboflux": TurboFlux,
@@ -403,4 +409,6 @@ PLUGINS = {
     "parallel_symbi": Parrllel_SymBi,
     "parallel_calig": Parallel_CaLiG,
     "calig": Parallel_CaLiG,
+    "parallel_newsp": CSMPP,
+    "newsp": CSMPP,
 }

@@ -62,8 +62,8 @@ void usage() {
           "    [--initial-time-limit S] [--orders ...] [-t N] [--auto-tuning 0|1]\n"
           "    [--mode batched|plain] [--batch N] [--device N] [--hash 0|1] [--turboflux-compat 0|1]\n"
           "    [--out per_update.csv]\n"
-          "algorithms: parallel_graphflow parallel_turboflux parallel_symbi parallel_calig\n"
-          "            (graphflow turboflux symbi calig alias them)\n");
+          "algorithms: parallel_graphflow parallel_turboflux parallel_symbi parallel_calig parallel_newsp\n"
+          "            (graphflow turboflux symbi calig newsp alias them)\n");
 }
 
 }  // namespace

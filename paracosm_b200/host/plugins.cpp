@@ -163,6 +163,8 @@ matching* make_plugin(const std::string& name, const EdgeList& q, const EdgeList
     return new Parrllel_SymBi(q, d, max_results, print_prep, print_enum, homo, opt);
   if (name == "parallel_calig" || name == "calig")
     return new Parallel_CaLiG(q, d, max_results, print_prep, print_enum, homo, opt);
+  if (name == "parallel_newsp" || name == "newsp")
+    return new CSMPP(q, d, max_results, print_prep, print_enum, homo, opt);
   return nullptr;
 }
 

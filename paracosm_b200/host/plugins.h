@@ -9,6 +9,8 @@
 //   parallel_symbi, symbi          -> CSM_ALGO_SYMBI     (DCS over a DAG of all query edges)
 //   parallel_calig, calig          -> CSM_ALGO_CALIG     (CaLiG-style lighting filter; the reference
 //                                     ships CaLiG as its own program, matching/Parallel_CaLiG)
+//   parallel_newsp, newsp          -> CSM_ALGO_NEWSP     (NewSP-style neighbour-label-frequency filter;
+//                                     the reference's own driver is matching/Parallel_NewSP)
 // Differences from the reference, all deliberate:
 //   - errors never exit the process: the calls record a CSM_E* code, and
 //     error() / error_text() report the first one;
@@ -124,6 +126,17 @@ class Parallel_CaLiG : public matching {
   Parallel_CaLiG(const EdgeList& q, const EdgeList& d, size_t max_results, bool print_prep, bool print_enum,
                  bool homo, const GpuOptions& opt)
       : matching(q, d, max_results, print_prep, print_enum, homo, CSM_ALGO_CALIG, opt) {}
+};
+
+// NewSP's CSMPP (ParaCOSM/CSM/matching/Parallel_NewSP/matching/CSMPP.h:8-183),
+// run by its own driver in the reference (Parallel_NewSP/matching/main.cpp),
+// which takes the csm options and processes the stream with the sequential
+// semantics; behind this interface it takes the same inputs as the others.
+class CSMPP : public matching {
+ public:
+  CSMPP(const EdgeList& q, const EdgeList& d, size_t max_results, bool print_prep, bool print_enum, bool homo,
+        const GpuOptions& opt)
+      : matching(q, d, max_results, print_prep, print_enum, homo, CSM_ALGO_NEWSP, opt) {}
 };
 
 // Plugin for an -a name, or nullptr for an unknown name.

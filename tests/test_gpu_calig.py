@@ -179,3 +179,26 @@ def test_lighting_filter_after_vertex_updates(gen_dir):
     ok = (want["status"] == ST_OK) & ~_duplicates(w.vlabels, w.edges, s)
     assert np.array_equal(res["pos"][ok], want["pos"][ok])
     assert np.array_equal(res["neg"][ok], want["neg"][ok])
+
+
+@pytest.mark.parametrize("max_batch", [65536, 7])
+@pytest.mark.parametrize("case", ["mixed_2el", "zipf_8q", "homo"])
+def test_newsp_filter_levels_equal_the_oracle(case, max_batch):
+    """The NewSP-style plugin keeps the same two levels; its search filters by the first."""
+    g = load_golden(case)
+    homo = g["params"]["homo"]
+    s = g["stream"]
+    n = len(g["vl"])
+    with Engine("parallel_newsp", homo=homo, max_batch=max_batch, want_hash=True) as eng:
+        eng.set_query(g["qv"], g["qe"])
+        eng.load_graph(g["vl"], g["e"])
+        eng.build_index()
+        _same_levels(eng.index(), pyoracle.calig_index(g["qv"], g["qe"], g["vl"], g["e"], homo=homo,
+                                                       with_lit=False), n)
+        res = eng.run(s)
+        _same_levels(eng.index(), pyoracle.calig_index(g["qv"], g["qe"], g["vl"], g["e"], s, homo=homo,
+                                                       with_lit=False), n)
+    x = g["exp"]
+    assert np.array_equal(res["pos"], x["symbi_pos"]) and np.array_equal(res["neg"], x["symbi_neg"])
+    ok = res["status"] == ST_OK
+    assert np.array_equal(res["hash"][ok], x["symbi_hash"][ok])

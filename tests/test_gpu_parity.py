@@ -11,7 +11,7 @@ from paracosm_b200 import ST_CAPPED, ST_INVALID, ST_OK, ST_TIMED_OUT, UPDATE_DTY
 
 pytestmark = pytest.mark.gpu
 
-ALGOS = ["parallel_graphflow", "parallel_turboflux", "parallel_symbi"]
+ALGOS = ["parallel_graphflow", "parallel_turboflux", "parallel_symbi", "parallel_newsp"]
 
 
 def run_engine(qv, qe, vl, e, stream, algo="parallel_graphflow", **kw):

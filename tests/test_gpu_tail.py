@@ -12,7 +12,7 @@ from paracosm_b200 import ST_CAPPED, Engine, workload
 
 pytestmark = pytest.mark.gpu
 
-ALGOS = ["parallel_graphflow", "parallel_turboflux", "parallel_symbi", "parallel_calig"]
+ALGOS = ["parallel_graphflow", "parallel_turboflux", "parallel_symbi", "parallel_calig", "parallel_newsp"]
 
 
 def _run(algo, qv, qe, vl, e, stream, **kw):
