@@ -102,7 +102,9 @@ typedef struct csm_cfg {
   uint32_t tail_enumerate;    /* when only counts are wanted (want_hash 0, no match sets) the search
                                  counts the last positions of an order that share no query edge as a
                                  product of candidate counts (not in the reference); != 0 enumerates
-                                 them one by one instead.  Counts are the same; work_bytes differ */
+                                 them one by one instead.  Counts are the same (a product saturates at
+                                 2^58 per partial match, beyond any count an enumeration reaches);
+                                 work_bytes differ */
 } csm_cfg;
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */
