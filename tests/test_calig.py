@@ -107,3 +107,21 @@ def test_skip_rule_on_a_small_stream(tmp_path):
     vl, e = workload.read_calig_graph(tmp_path / "d")
     got = pyoracle.run(qv, qe, vl, e, _without(workload.read_calig_stream(tmp_path / "s"), skip), want_hash=False)
     assert got["pos"].tolist() == [0, 0, 0, 2, 4, 0]
+
+
+def test_calig_program_options_without_a_gpu(tmp_path):
+    """-c limits the stream as the reference's inputUpdate does; a record with one
+    negative id is refused with a message and a nonzero exit."""
+    (tmp_path / "q").write_text("v 0 1\nv 1 1\nv 2 1\ne 0 1\ne 1 2\n")
+    (tmp_path / "d").write_text("v 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1\ne 2 3\n")
+    (tmp_path / "s").write_text("e 0 2\ne 1 3\ne -1 -4\ne 0 3\n")
+    base = [str(CALIG_BIN), "-d", str(tmp_path / "d"), "-q", str(tmp_path / "q"), "-s", str(tmp_path / "s")]
+    r = subprocess.run(base + ["-c", "2", "--skip-mask", str(tmp_path / "m")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "m").read_text().split() == ["0", "0"]
+    r = subprocess.run(base + ["--skip-mask", str(tmp_path / "m")], capture_output=True, text=True)
+    assert r.returncode == 0 and len((tmp_path / "m").read_text().split()) == 4
+    (tmp_path / "s2").write_text("e 0 2\ne -1 3\n")
+    r = subprocess.run(base[:5] + ["-s", str(tmp_path / "s2"), "--skip-mask", str(tmp_path / "m")],
+                       capture_output=True, text=True)
+    assert r.returncode != 0 and "mixed-sign" in r.stderr
