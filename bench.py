@@ -65,9 +65,9 @@ CONFIGS = {
         "preset": "c5", "algo": "parallel_symbi", "batch": 8192, "max_results": 1_000_000,
         "min_updates": 500_000, "deadline_ns": 1_000_000_000,
         "workload": "RMAT 2^24 V, avg deg 32 (268M edges), 32 vlabels Zipf(1.0), 4 elabels; 24- and 32-vertex "
-                    "queries (sparse and dense) as four standing queries on one graph, plugins SymBi / TurboFlux / "
-                    "GraphFlow round-robin (the CaLiG- and NewSP-style plugins are not built); 90/10 insert/delete "
-                    "stream; per update max_results 1e6 and a 1 s limit",
+                    "queries (sparse and dense) as four standing queries on one graph, plugins CaLiG-style / "
+                    "TurboFlux / SymBi / CaLiG-style; 90/10 insert/delete stream; per update max_results 1e6 and a "
+                    "1 s limit",
     },
     "c1": {
         "preset": "c1", "algo": "parallel_graphflow", "batch": 2000, "max_results": 0, "min_updates": 2000,
