@@ -21,7 +21,18 @@
 // counts and match-set hashes without printing.  --orders is accepted and
 // ignored (the engine derives its own orders).
 // Files may also be the generator's binary CSMG / CSMU containers.
+//
+// -q may name a directory: every file in it (names not starting with '.',
+// in name order) is a query on the same data graph, as in NewSP's
+// multi-query build (ParaCOSM/CSM/matching/Parallel_NewSP/graph/graph.cpp:550-574).
+// The first is the plugin's own query, the others are attached as standing
+// queries with the same plugin and cap; each update's counts are summed over
+// all queries.  --print-enum and the per-update hash cover the first query.
+#include <dirent.h>
 #include <sys/resource.h>
+#include <sys/stat.h>
+
+#include <algorithm>
 
 #include <chrono>
 #include <cstdio>
@@ -120,7 +131,27 @@ int main(int argc, char** argv) {
   printf("----------- Loading graphs ------------\n");
   EdgeList query, data;
   std::string err;
-  if (!load_graph_any(query_path, query, err)) { printf("%s\n", err.c_str()); return 1; }
+  struct stat qs;
+  if (stat(query_path.c_str(), &qs) == 0 && S_ISDIR(qs.st_mode)) {
+    std::vector<std::string> names;
+    if (DIR* dir = opendir(query_path.c_str())) {
+      while (dirent* e = readdir(dir))
+        if (e->d_name[0] != '.') names.push_back(query_path + "/" + e->d_name);
+      closedir(dir);
+    }
+    std::sort(names.begin(), names.end());
+    if (names.empty()) { printf("no query files in %s\n", query_path.c_str()); return 1; }
+    for (size_t i = 0; i < names.size(); i++) {
+      EdgeList q;
+      if (!load_graph_any(names[i], q, err)) { printf("%s\n", err.c_str()); return 1; }
+      if (i == 0) query = q;
+      else opt.more_queries.push_back(q);
+    }
+    printf("Load query graph number: %zu\n", names.size());
+  } else if (!load_graph_any(query_path, query, err)) {
+    printf("%s\n", err.c_str());
+    return 1;
+  }
   printf("# vertices = %u\n# edges = %llu\n", query.n, (unsigned long long)query.num_edges());
   if (!load_graph_any(initial_path, data, err)) { printf("%s\n", err.c_str()); return 1; }
   printf("# vertices = %u\n# edges = %llu\n", data.n, (unsigned long long)data.num_edges());

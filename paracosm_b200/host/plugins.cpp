@@ -32,6 +32,7 @@ matching::matching(const EdgeList& query, const EdgeList& data, size_t max_num_r
 }
 
 matching::~matching() {
+  for (csm_ctx* a : attached_) csm_gpu_destroy(a);
   if (ctx_) csm_gpu_destroy(ctx_);
 }
 
@@ -51,8 +52,29 @@ void matching::Preprocessing() {
   if (check(csm_gpu_set_query(ctx_, query_.n, query_.vlabels.data(), (uint32_t)query_.num_edges(),
                               query_.edges.data())))
     return;
+  if (!opt_.more_queries.empty()) {  // every query's labels stay distinct in the shared graph
+    std::vector<uint32_t> vl, el;
+    for (const EdgeList& q : opt_.more_queries) {
+      vl.insert(vl.end(), q.vlabels.begin(), q.vlabels.end());
+      for (uint64_t i = 0; i < q.num_edges(); i++) el.push_back(q.edges[3 * i + 2]);
+    }
+    if (check(csm_gpu_reserve_labels(ctx_, (uint32_t)vl.size(), vl.data(), (uint32_t)el.size(), el.data()))) return;
+  }
   if (check(csm_gpu_load_graph(ctx_, data_.n, data_.vlabels.data(), data_.num_edges(), data_.edges.data()))) return;
-  check(csm_gpu_build_index(ctx_));
+  if (check(csm_gpu_build_index(ctx_))) return;
+  for (const EdgeList& q : opt_.more_queries) {
+    csm_cfg c;
+    csm_gpu_default_cfg(&c);
+    c.algorithm = algo_;
+    c.max_results = (max_num_results_ >= 0xffffffffull) ? 0 : (uint64_t)max_num_results_;
+    c.want_hash = opt_.want_hash ? 1 : 0;
+    c.warps_per_block = opt_.warps_per_block;
+    c.blocks_per_sm = opt_.blocks_per_sm;
+    csm_ctx* a = nullptr;
+    if (check(csm_gpu_attach_query(ctx_, &c, q.n, q.vlabels.data(), (uint32_t)q.num_edges(), q.edges.data(), &a)))
+      return;
+    attached_.push_back(a);
+  }
   if (print_preprocessing_results_ && !err_ && algo_ != CSM_ALGO_GRAPHFLOW) {
     csm_index_info info;
     if (!check(csm_gpu_index_info(ctx_, &info))) {
@@ -77,6 +99,27 @@ void matching::InitialMatching() {
   if (err_) return;
   uint64_t c = 0;
   if (!check(csm_gpu_initial_match(ctx_, &c))) num_initial_results_ += c;
+  for (csm_ctx* a : attached_) {
+    c = 0;
+    if (check(csm_gpu_initial_match(a, &c))) return;
+    num_initial_results_ += c;
+  }
+}
+
+// Adds the attached queries' results for sequence numbers first .. first+n-1
+// to out (counts summed, the largest status kept).
+int matching::add_attached(uint64_t first, size_t n, csm_result* out) {
+  if (attached_.empty()) return CSM_OK;
+  std::vector<csm_result> r(n);
+  for (csm_ctx* a : attached_) {
+    if (check(csm_gpu_results(a, first, n, r.data()))) return err_;
+    for (size_t i = 0; i < n; i++) {
+      out[i].pos += r[i].pos;
+      out[i].neg += r[i].neg;
+      out[i].status = std::max(out[i].status, r[i].status);
+    }
+  }
+  return CSM_OK;
 }
 
 void matching::run_one(const Update& u) {
@@ -87,6 +130,7 @@ void matching::run_one(const Update& u) {
   const uint64_t first = seq_++;
   csm_result r;
   if (check(csm_gpu_results(ctx_, first, 1, &r))) return;
+  if (add_attached(first, 1, &r)) return;
   num_positive_results_ += r.pos;
   num_negative_results_ += r.neg;
 }
@@ -120,6 +164,7 @@ int matching::ProcessUpdates(const std::vector<Update>& ups, std::vector<csm_res
   const uint64_t first = seq_;
   seq_ += ups.size();
   if (check(csm_gpu_results(ctx_, first, ups.size(), out.data()))) return err_;
+  if (add_attached(first, ups.size(), out.data())) return err_;
   for (const csm_result& r : out) {
     num_positive_results_ += r.pos;
     num_negative_results_ += r.neg;

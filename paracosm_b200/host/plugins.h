@@ -43,6 +43,11 @@ struct GpuOptions {
   uint64_t deadline_ns = 0;
   uint32_t enum_capacity = 0;  // > 0: keep embeddings for PrintMatches (the reference's --print-enum)
   bool graphs = false;         // replay each batch size's launch sequence as a CUDA graph
+  // further queries on the same data graph (NewSP's multi-query build reads a
+  // directory of queries, ParaCOSM/CSM/matching/Parallel_NewSP/graph/graph.cpp:550-574);
+  // each is attached as a standing query with this plugin's settings and the
+  // per-update counts are summed over all queries
+  std::vector<EdgeList> more_queries;
 };
 
 class matching {
@@ -82,6 +87,7 @@ class matching {
  protected:
   int check(int rc);
   void run_one(const Update& u);
+  int add_attached(uint64_t first, size_t n, csm_result* out);
 
   const EdgeList& query_;
   const EdgeList& data_;
@@ -90,6 +96,7 @@ class matching {
   int algo_;
   GpuOptions opt_;
   csm_ctx* ctx_ = nullptr;
+  std::vector<csm_ctx*> attached_;  // contexts of opt_.more_queries
   size_t num_initial_results_ = 0, num_positive_results_ = 0, num_negative_results_ = 0;
   uint64_t seq_ = 0;  // sequence number of the next submitted update
   int err_ = CSM_OK;

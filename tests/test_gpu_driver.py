@@ -52,3 +52,37 @@ def test_driver_print_enum_lists_every_embedding():
     rows = [x for x in rows if len(x) == nq]
     x = g["exp"]
     assert len(rows) == int((x["symbi_pos"] + x["symbi_neg"]).sum())
+
+
+@pytest.mark.parametrize("algo", ["parallel_newsp", "parallel_symbi"])
+def test_driver_query_directory_sums_every_query(tmp_path, gen_dir, algo):
+    """-q DIR (NewSP's multi-query build): each file is a standing query on the same
+    data graph, and each update's counts are the sum over the queries."""
+    import shutil
+
+    from oracle import pyoracle
+    from paracosm_b200 import workload
+    w = workload.generate("c2", gen_dir / f"multiq_{algo}", extra=[
+        "--log2-n", "11", "--avg-degree", "6", "--vlabels", "3", "--zipf", "0", "--elabels", "2", "--updates", "300",
+        "--insert-frac", "0.8", "--seed", "21", "--query", "5:sparse:1", "--query", "4:dense", "--text"])
+    qdir = tmp_path / "queries"
+    qdir.mkdir()
+    for i in range(2):
+        shutil.copy(w.query_path(i), qdir / f"q{i}.graph")
+    out = tmp_path / "per_update.csv"
+    r = subprocess.run([str(CSM), "-q", str(qdir), "-d", str(w.directory / "data.graph"), "-u",
+                        str(w.directory / "stream.txt"), "-a", algo, "--batch", "64", "--out", str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    assert "Load query graph number: 2" in r.stdout
+    want_pos = np.zeros(len(w.stream), np.uint64)
+    want_neg = np.zeros(len(w.stream), np.uint64)
+    for qv, qe in w.queries:
+        ref = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream, want_hash=False)
+        want_pos += ref["pos"]
+        want_neg += ref["neg"]
+    rows = list(csv.DictReader(open(out)))
+    assert np.array_equal(np.array([int(x["pos"]) for x in rows], dtype=np.uint64), want_pos)
+    assert np.array_equal(np.array([int(x["neg"]) for x in rows], dtype=np.uint64), want_neg)
+    assert f"{int(want_pos.sum())} positive matches." in r.stdout.splitlines()
+    assert want_pos.sum() > 0
