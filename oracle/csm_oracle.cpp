@@ -883,6 +883,13 @@ void pack_bits(const std::vector<std::vector<char>>& f, uint64_t words, uint64_t
 
 }  // namespace
 
+extern "C" uint64_t oracle_group_assignments(uint32_t g, const uint64_t* N, int homo) {
+  if (g == 0 || g > kTailGroup) return 0;
+  uint64_t n[1u << kTailGroup] = {0};
+  for (uint32_t M = 1; M < (1u << g); M++) n[M] = N[M];
+  return group_assignments(g, n, homo != 0);
+}
+
 extern "C" int oracle_calig_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const uint32_t* q_edges,
                                   uint32_t n_v, const uint32_t* vlabels, uint64_t n_e, const uint32_t* edges,
                                   uint64_t n_up, const oracle_update* ups, int homo, uint64_t words, uint64_t* li0_out,

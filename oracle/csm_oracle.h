@@ -97,6 +97,12 @@ int oracle_index(uint32_t n_qv, const uint32_t* q_vlabels, uint32_t n_qe, const 
                  uint64_t n_up, const oracle_update* ups, int algo, uint32_t* root, uint32_t* order,
                  uint32_t* parents, uint64_t words, uint64_t* d1, uint64_t* d2);
 
+/* Injective assignments of a group of g <= 3 same-label tail positions (the
+ * counting search's group count), from N[M] = the number of candidates whose
+ * membership set over the group is exactly M (N[0] unused); without
+ * injectivity under homo.  Saturates at 2^58. */
+uint64_t oracle_group_assignments(uint32_t g, const uint64_t* N, int homo);
+
 /* CaLiG-style candidate flags on the graph after the first n_up updates, as
  * [n_qv][words] bitsets (any output may be null):
  *   li0: L(v) = L(u) and v has, per (vertex label, edge label) pair of u's

@@ -47,6 +47,8 @@ def lib() -> C.CDLL:
         _lib.oracle_initial_count.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                               C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
                                               C.POINTER(C.c_uint64)]
+        _lib.oracle_group_assignments.restype = C.c_uint64
+        _lib.oracle_group_assignments.argtypes = [C.c_uint32, C.c_void_p, C.c_int]
         _lib.oracle_calig_index.restype = C.c_int
         _lib.oracle_calig_index.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                             C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_uint64,
@@ -148,6 +150,15 @@ def index(q_vlabels, q_edges, vlabels, edges, updates=None, *, algo: str = "symb
     bits = lambda a: np.unpackbits(a.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)  # noqa: E731
     par = [[p for p in range(len(qv)) if (int(parents[q]) >> p) & 1] for q in range(len(qv))]
     return {"root": int(root.value), "order": order.tolist(), "parents": par, "d1": bits(d1), "d2": bits(d2)}
+
+
+def group_assignments(g: int, classes: dict, homo: bool = False) -> int:
+    """Injective assignments of g same-label tail positions; classes maps a
+    membership bitmask M to the number of candidates with exactly that membership."""
+    n = np.zeros(8, dtype=np.uint64)
+    for m, c in classes.items():
+        n[m] = c
+    return int(lib().oracle_group_assignments(g, _p(n), int(homo)))
 
 
 def calig_index(q_vlabels, q_edges, vlabels, edges, updates=None, *, homo: bool = False,

@@ -209,3 +209,23 @@ def test_oracle_tail_counting_with_groups_of_three(gen_dir, spec):
     assert np.array_equal(tail["pos"], full["pos"]) and np.array_equal(tail["neg"], full["neg"])
     assert np.array_equal(tail["status"], full["status"])
     assert full["pos"].sum() > 0
+
+
+def test_group_assignments_equal_brute_force():
+    """The counting search's group count against an explicit enumeration of injective
+    (and, under homomorphism, arbitrary) assignments on random candidate sets."""
+    import itertools
+    rng = np.random.default_rng(7)
+    for _ in range(300):
+        g = int(rng.integers(1, 4))
+        universe = int(rng.integers(1, 9))
+        sets = [set(np.nonzero(rng.random(universe) < 0.5)[0].tolist()) for _ in range(g)]
+        classes = {}
+        for x in range(universe):
+            m = sum(1 << i for i in range(g) if x in sets[i])
+            if m:
+                classes[m] = classes.get(m, 0) + 1
+        inj = sum(1 for t in itertools.product(*[sorted(s) for s in sets]) if len(set(t)) == g)
+        anyway = int(np.prod([len(s) for s in sets]))
+        assert pyoracle.group_assignments(g, classes) == inj, (sets, classes)
+        assert pyoracle.group_assignments(g, classes, homo=True) == anyway
