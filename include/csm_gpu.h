@@ -60,7 +60,7 @@ extern "C" {
 #define CSM_ALGO_TURBOFLUX 1 /* -a parallel_turboflux / turboflux: DCG over a query spanning tree */
 #define CSM_ALGO_SYMBI 2     /* -a parallel_symbi / symbi: DCS over a DAG of all query edges */
 #define CSM_ALGO_CALIG 3     /* -a parallel_calig / calig: CaLiG-style lighting filter over every query edge;
-                                an insertion of a present edge counts 0 (Parallel_CaLiG/parallel_calig.cpp:1233) */
+                                an insertion of a present edge counts 0 (Parallel_CaLiG/parallel_calig.cpp:1249) */
 #define CSM_ALGO_NEWSP 4     /* -a parallel_newsp / newsp: NewSP-style neighbour-label-frequency filter
                                 (Parallel_NewSP/matching/CSMPP.cpp:81-113 indexCheck); leaf vertices counted
                                 together when only counts are wanted (its isolated vertices, :641) */

@@ -9,11 +9,11 @@
 // The file formats are CaLiG's own (matching/CaLiG/README.md): `v id label`,
 // `e a b` without edge labels; a stream of `e a b` insertions.  The
 // reference reads stream ids as unsigned integers, so its deletion records
-// (`e -a-1 -b-1`) never reach its deletion branch (parallel_calig.cpp:1224
+// (`e -a-1 -b-1`) never reach its deletion branch (parallel_calig.cpp:1228
 // tests `v1 < 0` on an unsigned value); such records are refused here.
 //
 // The update loop is the insertion branch of updateAndMatching
-// (parallel_calig.cpp:1214-1265), with the count of each update written out
+// (parallel_calig.cpp:1214-1272), with the count of each update written out
 // instead of summed: an update whose endpoint has a label the query does not
 // use, an edge already present, or one that turnOnProcess_safe classifies as
 // safe counts 0; otherwise the lighting index is updated

@@ -52,7 +52,7 @@ __global__ void k_seed(uint32_t B, const UpdInfo* info, DevGraph g, const Plan* 
   const UpdInfo u = info[s];
   uint32_t sf = 1;
   // dup_zero: an insertion of a present edge counts nothing (CaLiG skips it,
-  // ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:1233)
+  // ParaCOSM/CSM/matching/Parallel_CaLiG/parallel_calig.cpp:1249)
   if ((u.flags & UF_VALID) && !(u.flags & UF_INVALID) && !(dup_zero && (u.flags & UF_DUP))) {
     const uint32_t L1 = g.vlabel[u.v1], L2 = g.vlabel[u.v2], l = u.label;
     const uint32_t na = plan->n_anchor;

@@ -24,7 +24,7 @@ bool load_calig_stream(const std::string& path, std::vector<Update>& s, std::str
 bool save_calig_graph(const std::string& path, const EdgeList& g);
 bool save_calig_stream(const std::string& path, const std::vector<Update>& s);
 
-// The reference's insertion loop (updateAndMatching, :1214-1265) skips an
+// The reference's insertion loop (updateAndMatching, :1214-1272) skips an
 // insertion when turnOnProcess_safe (:774-802) finds no candidate-neighbour
 // entry at its first endpoint.  Such entries exist at a vertex that had a
 // neighbour with a query label in the initial graph, and appear at a vertex

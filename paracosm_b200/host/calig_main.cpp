@@ -1,5 +1,5 @@
 // calig: the reference's CaLiG program (ParaCOSM/CSM/matching/Parallel_CaLiG/
-// parallel_calig.cpp:1414-1490) over the CUDA engine.
+// parallel_calig.cpp:1414-1481) over the CUDA engine.
 //
 //   calig -d data -q query -s stream [-c max_updates] [-t threads]
 //     engine options (not in the reference):
@@ -18,7 +18,7 @@
 // unsigned 32-bit value (numAdd / searchCore return uint, :1014, :1062).
 // --compat 0 counts every insertion exactly.  Deletion records, which the
 // reference reads but cannot process (it compares an unsigned id with 0,
-// :1224), are processed here: each counts the embeddings it destroys, before
+// :1228), are processed here: each counts the embeddings it destroys, before
 // removing the edge.  --skip-mask FILE writes the --compat skip decision of
 // each update (one 0/1 per line) and exits without using the GPU.
 #include <chrono>
