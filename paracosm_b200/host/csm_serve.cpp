@@ -1,7 +1,7 @@
 // csm_serve: the serving loop (serve.h) as a command-line tool.
 //
 //   csm_serve -w WORKLOAD_DIR [--queries N] [--rate R] [--max-batch B] [--budget-gb G]
-//             [--cap N] [--plugins symbi,turboflux,graphflow] [--arrive-every S]
+//             [--cap N] [--plugins symbi,turboflux,graphflow,calig,newsp] [--arrive-every S]
 //             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]
 //             [--deadline-ms MS] [--device D]
 //             [--out results.bin]
@@ -31,6 +31,8 @@ int plugin_of(const std::string& s) {
   if (s.find("turboflux") != std::string::npos) return CSM_ALGO_TURBOFLUX;
   if (s.find("symbi") != std::string::npos) return CSM_ALGO_SYMBI;
   if (s.find("graphflow") != std::string::npos) return CSM_ALGO_GRAPHFLOW;
+  if (s.find("calig") != std::string::npos) return CSM_ALGO_CALIG;
+  if (s.find("newsp") != std::string::npos) return CSM_ALGO_NEWSP;
   return -1;
 }
 
