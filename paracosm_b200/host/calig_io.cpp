@@ -4,8 +4,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
-#include <sstream>
 #include <unordered_set>
 
 namespace csm {
@@ -13,24 +11,68 @@ namespace {
 
 uint64_t edge_key(uint32_t a, uint32_t b) { return ((uint64_t)std::min(a, b) << 32) | std::max(a, b); }
 
+bool slurp(const std::string& path, std::string& buf) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) return false;
+  fseek(f, 0, SEEK_END);
+  const long sz = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  buf.resize(sz > 0 ? (size_t)sz : 0);
+  const size_t got = sz > 0 ? fread(&buf[0], 1, (size_t)sz, f) : 0;
+  fclose(f);
+  return got == buf.size();
+}
+
+// Whitespace-separated tokens of a whole file: words and signed integers.
+struct Scan {
+  const char* p;
+  const char* e;
+  bool skip() {
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r')) p++;
+    return p < e;
+  }
+  bool word(std::string& w) {
+    if (!skip()) return false;
+    const char* s = p;
+    while (p < e && !(*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r')) p++;
+    w.assign(s, (size_t)(p - s));
+    return true;
+  }
+  bool int64(int64_t& v) {
+    if (!skip()) return false;
+    bool neg = false;
+    if (*p == '-' || *p == '+') { neg = *p == '-'; p++; }
+    if (p >= e || *p < '0' || *p > '9') return false;
+    int64_t x = 0;
+    while (p < e && *p >= '0' && *p <= '9') {
+      x = x * 10 + (*p - '0');
+      if (x > (1LL << 40)) return false;
+      p++;
+    }
+    v = neg ? -x : x;
+    return true;
+  }
+};
+
 }  // namespace
 
 bool load_calig_graph(const std::string& path, EdgeList& g, std::string& err) {
-  std::ifstream f(path);
-  if (!f) { err = "Fail to open graph file: " + path; return false; }
+  std::string buf;
+  if (!slurp(path, buf)) { err = "Fail to open graph file: " + path; return false; }
+  Scan sc{buf.data(), buf.data() + buf.size()};
   g = EdgeList{};
   std::string tag;
   std::vector<int64_t> raw;
-  while (f >> tag) {
+  while (sc.word(tag)) {
     if (tag == "v") {
       int64_t id, lb;
-      if (!(f >> id >> lb) || id < 0) { err = "bad vertex line in " + path; return false; }
+      if (!sc.int64(id) || !sc.int64(lb) || id < 0) { err = "bad vertex line in " + path; return false; }
       if (lb < 0) lb = 0;  // inputQ: a label of -1 is read as 0
       if ((uint64_t)id >= g.vlabels.size()) g.vlabels.resize((size_t)id + 1, kNotExist);
       g.vlabels[(size_t)id] = (uint32_t)lb;
     } else if (tag == "e") {
       int64_t a, b;
-      if (!(f >> a >> b)) { err = "bad edge line in " + path; return false; }
+      if (!sc.int64(a) || !sc.int64(b)) { err = "bad edge line in " + path; return false; }
       raw.push_back(a); raw.push_back(b);
     } else {
       err = "unexpected token '" + tag + "' in " + path;
@@ -49,12 +91,14 @@ bool load_calig_graph(const std::string& path, EdgeList& g, std::string& err) {
 }
 
 bool load_calig_stream(const std::string& path, std::vector<Update>& s, std::string& err, uint64_t max_updates) {
-  std::ifstream f(path);
-  if (!f) { err = "Fail to open stream file: " + path; return false; }
+  std::string buf;
+  if (!slurp(path, buf)) { err = "Fail to open stream file: " + path; return false; }
+  Scan sc{buf.data(), buf.data() + buf.size()};
   s.clear();
   std::string tag;
   int64_t a, b;
-  while (f >> tag >> a >> b) {
+  while (sc.word(tag)) {
+    if (!sc.int64(a) || !sc.int64(b)) { err = "bad update line in " + path; return false; }
     if (max_updates && s.size() >= max_updates) break;  // -c (inputUpdate, :1201-1212)
     Update u{};
     u.type = 'e';
