@@ -57,17 +57,30 @@ bool has_magic(const std::string& path, const char* magic) {
 }  // namespace
 
 void canonicalize(EdgeList& g) {
-  std::vector<uint32_t> out;
-  out.reserve(g.edges.size());
-  std::unordered_set<uint64_t> seen;
-  seen.reserve(g.num_edges() * 2 + 16);
-  uint32_t max_el = 0;
-  for (uint64_t i = 0; i < g.num_edges(); i++) {
-    uint32_t a = g.edges[3 * i], b = g.edges[3 * i + 1], l = g.edges[3 * i + 2];
+  // sort (undirected key, position) pairs: the first occurrence of each edge
+  // keeps its label; 16 bytes per edge instead of a hash set's nodes
+  struct KI { uint64_t key; uint64_t idx; };
+  const uint64_t m = g.num_edges();
+  std::vector<KI> ki;
+  ki.reserve(m);
+  for (uint64_t i = 0; i < m; i++) {
+    const uint32_t a = g.edges[3 * i], b = g.edges[3 * i + 1];
     if (a == b) continue;
-    uint64_t key = ((uint64_t)std::min(a, b) << 32) | std::max(a, b);
-    if (!seen.insert(key).second) continue;
-    out.push_back(a); out.push_back(b); out.push_back(l);
+    ki.push_back(KI{((uint64_t)std::min(a, b) << 32) | std::max(a, b), i});
+  }
+  std::sort(ki.begin(), ki.end(), [](const KI& x, const KI& y) { return x.key != y.key ? x.key < y.key : x.idx < y.idx; });
+  std::vector<uint64_t> keep;
+  keep.reserve(ki.size());
+  for (size_t j = 0; j < ki.size(); j++)
+    if (j == 0 || ki[j].key != ki[j - 1].key) keep.push_back(ki[j].idx);
+  std::vector<KI>().swap(ki);
+  std::sort(keep.begin(), keep.end());  // file order
+  std::vector<uint32_t> out;
+  out.reserve(3 * keep.size());
+  uint32_t max_el = 0;
+  for (uint64_t i : keep) {
+    const uint32_t l = g.edges[3 * i + 2];
+    out.push_back(g.edges[3 * i]); out.push_back(g.edges[3 * i + 1]); out.push_back(l);
     max_el = std::max(max_el, l + 1);
   }
   g.edges.swap(out);

@@ -40,3 +40,16 @@ def test_serve_tool_usage():
         assert opt in r.stderr
     r = subprocess.run([str(serve)], capture_output=True, text=True)
     assert r.returncode == 2
+
+
+def test_loaders_drop_self_loops_and_duplicate_edges(tmp_path):
+    """Edges are kept once, the first occurrence winning (Graph::AddEdge is a no-op on an
+    existing edge, ParaCOSM/CSM/graph/graph.cpp:63-64); self loops are dropped.  The csm
+    driver prints the loaded sizes before it needs a GPU."""
+    (tmp_path / "q").write_text("v 0 0\nv 1 0\ne 0 1 0\n")
+    (tmp_path / "d").write_text("v 0 0\nv 1 0\nv 2 0\ne 0 1 5\ne 1 0 6\ne 1 2 0\ne 2 2 0\ne 0 1 7\ne 2 0 1\n")
+    (tmp_path / "s").write_text("e 0 2 0\n")
+    r = subprocess.run([str(CSM), "-q", str(tmp_path / "q"), "-d", str(tmp_path / "d"), "-u", str(tmp_path / "s"),
+                        "-a", "parallel_symbi"], capture_output=True, text=True, timeout=120)
+    sizes = [ln for ln in r.stdout.splitlines() if ln.startswith("# edges = ")]
+    assert sizes[:2] == ["# edges = 1", "# edges = 3"], r.stdout
