@@ -3,7 +3,6 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
-#include <unordered_set>
 
 namespace csm {
 namespace {
