@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -54,26 +55,32 @@ int main(int argc, char** argv) {
   size_t thread_num = 32;
   bool compat = true;
   GpuOptions opt;
-  for (int i = 1; i < argc; i++) {
-    const std::string k = argv[i];
-    auto val = [&]() -> std::string {
-      if (i + 1 >= argc) { usage(); exit(2); }
-      return argv[++i];
-    };
-    if (k == "-d") g_path = val();
-    else if (k == "-q") q_path = val();
-    else if (k == "-s") s_path = val();
-    else if (k == "-c") cnum = std::stoull(val());
-    else if (k == "-t") thread_num = std::stoul(val());
-    else if (k == "--compat") compat = val() != "0";
-    else if (k == "--mode") opt.mode = val() == "plain" ? CSM_MODE_PLAIN : CSM_MODE_BATCHED;
-    else if (k == "--batch") opt.max_batch = (uint32_t)std::stoul(val());
-    else if (k == "--device") opt.device = std::stoi(val());
-    else if (k == "--max-results") max_results = std::stoull(val());
-    else if (k == "--out") out_path = val();
-    else if (k == "--skip-mask") mask_path = val();
-    else if (k == "-h" || k == "--help") { usage(); return 0; }
-    else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+  try {  // a malformed number ends the run with the usage text, as an unknown option does
+    for (int i = 1; i < argc; i++) {
+      const std::string k = argv[i];
+      auto val = [&]() -> std::string {
+        if (i + 1 >= argc) { usage(); exit(2); }
+        return argv[++i];
+      };
+      if (k == "-d") g_path = val();
+      else if (k == "-q") q_path = val();
+      else if (k == "-s") s_path = val();
+      else if (k == "-c") cnum = std::stoull(val());
+      else if (k == "-t") thread_num = std::stoul(val());
+      else if (k == "--compat") compat = val() != "0";
+      else if (k == "--mode") opt.mode = val() == "plain" ? CSM_MODE_PLAIN : CSM_MODE_BATCHED;
+      else if (k == "--batch") opt.max_batch = (uint32_t)std::stoul(val());
+      else if (k == "--device") opt.device = std::stoi(val());
+      else if (k == "--max-results") max_results = std::stoull(val());
+      else if (k == "--out") out_path = val();
+      else if (k == "--skip-mask") mask_path = val();
+      else if (k == "-h" || k == "--help") { usage(); return 0; }
+      else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+    }
+  } catch (const std::exception&) {
+    fprintf(stderr, "bad option value\n");
+    usage();
+    return 2;
   }
   if (g_path.empty() || q_path.empty() || s_path.empty()) { usage(); return 2; }
 

@@ -40,6 +40,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -86,34 +87,40 @@ int main(int argc, char** argv) {
   bool print_prep = true, print_enum = false, homo = false, report_initial = true;
   size_t thread_num = 6, auto_tuning = 1;
   GpuOptions opt;
-  for (int i = 1; i < argc; i++) {
-    const std::string k = argv[i];
-    auto val = [&]() -> std::string {
-      if (i + 1 >= argc) { usage(); exit(2); }
-      return argv[++i];
-    };
-    if (k == "-q" || k == "--query") query_path = val();
-    else if (k == "-d" || k == "--data") initial_path = val();
-    else if (k == "-u" || k == "--update") stream_path = val();
-    else if (k == "-a" || k == "--algorithm") algorithm = val();
-    else if (k == "--max-results") max_num_results = std::stoull(val());
-    else if (k == "--time-limit") time_limit = std::stod(val());
-    else if (k == "--print-prep") print_prep = parse_bool(val());
-    else if (k == "--print-enum") print_enum = parse_bool(val());
-    else if (k == "--homo") homo = parse_bool(val());
-    else if (k == "--report-initial") report_initial = parse_bool(val());
-    else if (k == "--initial-time-limit") initial_time_limit = std::stod(val());
-    else if (k == "--orders") { while (i + 1 < argc && argv[i + 1][0] != '-') i++; }
-    else if (k == "-t" || k == "--thread-num") thread_num = std::stoul(val());
-    else if (k == "--auto-tuning") auto_tuning = std::stoul(val());
-    else if (k == "--mode") opt.mode = val() == "plain" ? CSM_MODE_PLAIN : CSM_MODE_BATCHED;
-    else if (k == "--batch") opt.max_batch = (uint32_t)std::stoul(val());
-    else if (k == "--device") opt.device = std::stoi(val());
-    else if (k == "--hash") opt.want_hash = parse_bool(val());
-    else if (k == "--turboflux-compat") opt.turboflux_compat = parse_bool(val());
-    else if (k == "--out") out_path = val();
-    else if (k == "-h" || k == "--help") { usage(); return 0; }
-    else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+  try {  // a malformed number ends the run with the usage text, as an unknown option does
+    for (int i = 1; i < argc; i++) {
+      const std::string k = argv[i];
+      auto val = [&]() -> std::string {
+        if (i + 1 >= argc) { usage(); exit(2); }
+        return argv[++i];
+      };
+      if (k == "-q" || k == "--query") query_path = val();
+      else if (k == "-d" || k == "--data") initial_path = val();
+      else if (k == "-u" || k == "--update") stream_path = val();
+      else if (k == "-a" || k == "--algorithm") algorithm = val();
+      else if (k == "--max-results") max_num_results = std::stoull(val());
+      else if (k == "--time-limit") time_limit = std::stod(val());
+      else if (k == "--print-prep") print_prep = parse_bool(val());
+      else if (k == "--print-enum") print_enum = parse_bool(val());
+      else if (k == "--homo") homo = parse_bool(val());
+      else if (k == "--report-initial") report_initial = parse_bool(val());
+      else if (k == "--initial-time-limit") initial_time_limit = std::stod(val());
+      else if (k == "--orders") { while (i + 1 < argc && argv[i + 1][0] != '-') i++; }
+      else if (k == "-t" || k == "--thread-num") thread_num = std::stoul(val());
+      else if (k == "--auto-tuning") auto_tuning = std::stoul(val());
+      else if (k == "--mode") opt.mode = val() == "plain" ? CSM_MODE_PLAIN : CSM_MODE_BATCHED;
+      else if (k == "--batch") opt.max_batch = (uint32_t)std::stoul(val());
+      else if (k == "--device") opt.device = std::stoi(val());
+      else if (k == "--hash") opt.want_hash = parse_bool(val());
+      else if (k == "--turboflux-compat") opt.turboflux_compat = parse_bool(val());
+      else if (k == "--out") out_path = val();
+      else if (k == "-h" || k == "--help") { usage(); return 0; }
+      else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+    }
+  } catch (const std::exception&) {
+    fprintf(stderr, "bad option value\n");
+    usage();
+    return 2;
   }
   if (query_path.empty() || initial_path.empty() || stream_path.empty()) {
     fprintf(stderr, "-q, -d and -u are required\n");

@@ -53,3 +53,11 @@ def test_loaders_drop_self_loops_and_duplicate_edges(tmp_path):
                         "-a", "parallel_symbi"], capture_output=True, text=True, timeout=120)
     sizes = [ln for ln in r.stdout.splitlines() if ln.startswith("# edges = ")]
     assert sizes[:2] == ["# edges = 1", "# edges = 3"], r.stdout
+
+
+def test_malformed_option_values_print_usage():
+    for tool, args in ((CSM, ["-q", "a", "-d", "b", "-u", "c", "--max-results", "many"]),
+                       (CSM.parent / "calig", ["-d", "a", "-q", "b", "-s", "c", "-c", "x"])):
+        r = subprocess.run([str(tool)] + args, capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2
+        assert "bad option value" in r.stderr
