@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 
 #include "calig_io.h"
@@ -36,34 +37,40 @@ int main(int argc, char** argv) {
   preset("c1", s);
   std::string out;
   bool text = false, calig = false, binary = true, queries_set = false;
-  for (int i = 1; i < argc; i++) {
-    std::string k = argv[i];
-    auto nxt = [&]() -> std::string { if (i + 1 >= argc) { usage(); exit(2); } return argv[++i]; };
-    if (k == "--preset") { if (!preset(nxt(), s)) { fprintf(stderr, "unknown preset\n"); return 2; } }
-    else if (k == "--out") out = nxt();
-    else if (k == "--seed") s.seed = std::stoull(nxt());
-    else if (k == "--text") text = true;
-    else if (k == "--calig") calig = true;
-    else if (k == "--no-binary") binary = false;
-    else if (k == "--log2-n") s.log2_n = (uint32_t)std::stoul(nxt());
-    else if (k == "--avg-degree") s.avg_degree = std::stod(nxt());
-    else if (k == "--vlabels") s.n_vlabels = (uint32_t)std::stoul(nxt());
-    else if (k == "--zipf") s.vlabel_zipf = std::stod(nxt());
-    else if (k == "--elabels") s.n_elabels = (uint32_t)std::stoul(nxt());
-    else if (k == "--updates") s.n_updates = std::stoull(nxt());
-    else if (k == "--insert-frac") s.insert_fraction = std::stod(nxt());
-    else if (k == "--holdout-frac") s.holdout_fraction = std::stod(nxt());
-    else if (k == "--query") {
-      if (!queries_set) { s.queries.clear(); queries_set = true; }
-      std::string v = nxt();
-      QuerySpec q;
-      char kind[16] = {0};
-      unsigned size = 0, extra = 0; double mindeg = 0;
-      int got = sscanf(v.c_str(), "%u:%15[a-z]:%u:%lf", &size, kind, &extra, &mindeg);
-      if (got < 2) { usage(); return 2; }
-      q.size = size; q.dense = strcmp(kind, "dense") == 0; q.extra_edges = extra; q.min_avg_degree = mindeg;
-      s.queries.push_back(q);
-    } else { usage(); return 2; }
+  try {  // a malformed number ends the run with the usage text, as an unknown option does
+    for (int i = 1; i < argc; i++) {
+      std::string k = argv[i];
+      auto nxt = [&]() -> std::string { if (i + 1 >= argc) { usage(); exit(2); } return argv[++i]; };
+      if (k == "--preset") { if (!preset(nxt(), s)) { fprintf(stderr, "unknown preset\n"); return 2; } }
+      else if (k == "--out") out = nxt();
+      else if (k == "--seed") s.seed = std::stoull(nxt());
+      else if (k == "--text") text = true;
+      else if (k == "--calig") calig = true;
+      else if (k == "--no-binary") binary = false;
+      else if (k == "--log2-n") s.log2_n = (uint32_t)std::stoul(nxt());
+      else if (k == "--avg-degree") s.avg_degree = std::stod(nxt());
+      else if (k == "--vlabels") s.n_vlabels = (uint32_t)std::stoul(nxt());
+      else if (k == "--zipf") s.vlabel_zipf = std::stod(nxt());
+      else if (k == "--elabels") s.n_elabels = (uint32_t)std::stoul(nxt());
+      else if (k == "--updates") s.n_updates = std::stoull(nxt());
+      else if (k == "--insert-frac") s.insert_fraction = std::stod(nxt());
+      else if (k == "--holdout-frac") s.holdout_fraction = std::stod(nxt());
+      else if (k == "--query") {
+        if (!queries_set) { s.queries.clear(); queries_set = true; }
+        std::string v = nxt();
+        QuerySpec q;
+        char kind[16] = {0};
+        unsigned size = 0, extra = 0; double mindeg = 0;
+        int got = sscanf(v.c_str(), "%u:%15[a-z]:%u:%lf", &size, kind, &extra, &mindeg);
+        if (got < 2) { usage(); return 2; }
+        q.size = size; q.dense = strcmp(kind, "dense") == 0; q.extra_edges = extra; q.min_avg_degree = mindeg;
+        s.queries.push_back(q);
+      } else { usage(); return 2; }
+    }
+  } catch (const std::exception&) {
+    fprintf(stderr, "bad option value\n");
+    usage();
+    return 2;
   }
   if (out.empty()) { usage(); return 2; }
   mkdir(out.c_str(), 0755);

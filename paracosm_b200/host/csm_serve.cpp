@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -67,33 +68,39 @@ int main(int argc, char** argv) {
   uint32_t nqueries = 0;
   double arrive_every = 0;
   ServeConfig cfg;
-  for (int i = 1; i < argc; i++) {
-    const std::string k = argv[i];
-    auto val = [&]() -> std::string {
-      if (i + 1 >= argc) { usage(); exit(2); }
-      return argv[++i];
-    };
-    if (k == "-w") wdir = val();
-    else if (k == "-d") dpath = val();
-    else if (k == "-u") upath = val();
-    else if (k == "-q") qspecs.push_back(val());
-    else if (k == "--queries") nqueries = (uint32_t)std::stoul(val());
-    else if (k == "--rate") cfg.rate = std::stod(val());
-    else if (k == "--max-batch") cfg.max_batch = (uint32_t)std::stoul(val());
-    else if (k == "--budget-gb") cfg.budget_bytes = (uint64_t)(std::stod(val()) * (double)(1ull << 30));
-    else if (k == "--cap") cap = std::stoull(val());
-    else if (k == "--plugins") plugins = split(val(), ',');
-    else if (k == "--arrive-every") arrive_every = std::stod(val());
-    else if (k == "--max-updates") max_updates = std::stoull(val());
-    else if (k == "--max-seconds") cfg.max_seconds = std::stod(val());
-    else if (k == "--seed") cfg.seed = std::stoull(val());
-    else if (k == "--hash") cfg.want_hash = std::stoi(val()) != 0;
-    else if (k == "--graphs") cfg.graphs = std::stoi(val()) != 0;
-    else if (k == "--deadline-ms") cfg.deadline_ns = (uint64_t)(std::stod(val()) * 1e6);
-    else if (k == "--device") cfg.device = std::stoi(val());
-    else if (k == "--out") out_path = val();
-    else if (k == "-h" || k == "--help") { usage(); return 0; }
-    else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+  try {  // a malformed number ends the run with the usage text, as an unknown option does
+    for (int i = 1; i < argc; i++) {
+      const std::string k = argv[i];
+      auto val = [&]() -> std::string {
+        if (i + 1 >= argc) { usage(); exit(2); }
+        return argv[++i];
+      };
+      if (k == "-w") wdir = val();
+      else if (k == "-d") dpath = val();
+      else if (k == "-u") upath = val();
+      else if (k == "-q") qspecs.push_back(val());
+      else if (k == "--queries") nqueries = (uint32_t)std::stoul(val());
+      else if (k == "--rate") cfg.rate = std::stod(val());
+      else if (k == "--max-batch") cfg.max_batch = (uint32_t)std::stoul(val());
+      else if (k == "--budget-gb") cfg.budget_bytes = (uint64_t)(std::stod(val()) * (double)(1ull << 30));
+      else if (k == "--cap") cap = std::stoull(val());
+      else if (k == "--plugins") plugins = split(val(), ',');
+      else if (k == "--arrive-every") arrive_every = std::stod(val());
+      else if (k == "--max-updates") max_updates = std::stoull(val());
+      else if (k == "--max-seconds") cfg.max_seconds = std::stod(val());
+      else if (k == "--seed") cfg.seed = std::stoull(val());
+      else if (k == "--hash") cfg.want_hash = std::stoi(val()) != 0;
+      else if (k == "--graphs") cfg.graphs = std::stoi(val()) != 0;
+      else if (k == "--deadline-ms") cfg.deadline_ns = (uint64_t)(std::stod(val()) * 1e6);
+      else if (k == "--device") cfg.device = std::stoi(val());
+      else if (k == "--out") out_path = val();
+      else if (k == "-h" || k == "--help") { usage(); return 0; }
+      else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
+    }
+  } catch (const std::exception&) {
+    fprintf(stderr, "bad option value\n");
+    usage();
+    return 2;
   }
   EdgeList data;
   std::vector<Update> stream;
