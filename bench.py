@@ -35,9 +35,9 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact counts"
-# DRAM bytes (read + write) of one k_search launch over a 4,096-update C3
-# batch, from the ncu capture summarised in profiles/k_search_c3_b4096.md;
-# scaled to a launch by the updates it processes.
+# DRAM bytes (read + write) of one search launch over a 4,096-update C3
+# batch, from an ncu capture of that launch (dram__bytes_read.sum +
+# dram__bytes_write.sum); scaled to a launch by the updates it processes.
 SEARCH_DRAM_BYTES_PER_4096 = 93.0e6
 
 CONFIGS = {
@@ -145,101 +145,209 @@ def cuda_view(ptr: int, nbytes: int, device: int):
     return torch.as_tensor(_Arr(), device=f"cuda:{device}")
 
 
-def get_workload(cfg: dict, n_updates: int):
+def stream_plan(cfg: dict, warmup: int, steps: int, e2e_steps: int = 2) -> tuple[int, int]:
+    """(stream length, first timed update): the same for the GPU arm and the reference arm, so
+    both generate one workload and time the same updates.  The first `warmup` batches are the
+    warm-up; the timed window starts at update warmup * batch."""
+    B = cfg["batch"]
+    return max(cfg["min_updates"], (warmup + max(steps, e2e_steps)) * B), warmup * B
+
+
+def bench_config(cfg: dict, args, world: int) -> dict:
+    """The `config` object of both arms' JSON lines (built by one function so that they match)."""
+    n_updates, first = stream_plan(cfg, args.warmup, args.steps, args.e2e_steps)
+    return {"workload": cfg["workload"], "plugin": cfg["algo"], "batch": cfg["batch"], "stream_updates": n_updates,
+            "first_timed_update": first, "updates_timed": args.steps * cfg["batch"],
+            "max_results": cfg["max_results"],
+            "tail": "enumerated" if args.tail_enumerate else "counted (independent tail of each order)",
+            "l2": "inputs larger than L2 (graph ~3.4 GB in HBM)",
+            "parallelism": f"seed-sharded x{world} (replicated graph, one all-reduce per batch)"
+            if world > 1 else "single GPU"}
+
+
+def get_workload(cfg: dict, n_updates: int, snapshot_at: int = 0):
+    """Seeded workload; with snapshot_at the generator also writes the data graph as it stands
+    after the first snapshot_at updates (data_at_<n>.bin), where runs of the reference start."""
     from paracosm_b200 import workload
     base = Path(os.environ.get("CSM_BENCH_DIR", "/tmp/csm_bench"))
     d = base / f"{cfg['preset']}_{n_updates}"
     t0 = time.perf_counter()
-    w = workload.generate(cfg["preset"], d, updates=n_updates)
+    extra = ["--snapshot-at", str(snapshot_at)] if snapshot_at else None
+    w = workload.generate(cfg["preset"], d, updates=n_updates, extra=extra)
     log(f"workload {d} ready in {time.perf_counter() - t0:.1f}s: {len(w.vlabels)} V, {len(w.edges)} E, "
         f"{len(w.stream)} updates")
     return w
 
 
-def ref_start(w, algo: str, threads: int, cap: int, budget_s: float):
-    """Starts the reference (oracle/_ref, built from the reference sources) on the stream.
-    Its watchdog ends the run after `budget_s` seconds of incremental matching even
-    inside an update (parallel TurboFlux ignores the result cap below depth 2)."""
-    drv = ROOT / "oracle" / "_ref" / "ref_driver"
-    if not drv.exists():
-        return None
-    out = Path(tempfile.mkdtemp()) / "ref.csv"
-    cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(w.directory / "data.bin"), "-U",
-           str(w.directory / "stream.bin"), "-a", algo, "-t", str(threads), "--wall-budget", str(budget_s),
-           "--out", str(out)]
-    if cap:
-        cmd += ["--max-results", str(cap)]
-    p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
-    return {"proc": p, "out": out, "algo": algo, "threads": threads, "budget": budget_s, "t0": time.perf_counter()}
+class RefRun:
+    """One run of the reference compiled from its sources (oracle/_ref/ref_driver: the unmodified
+    plugin objects driven in the sequential update order) over the stream from update `first`,
+    starting from the data graph as it stands there.  Gated runs load and preprocess at once
+    and start their timed update loop only when `go()` is called, so that timed loops never
+    overlap.  A watchdog ends a run `budget` seconds into its update loop, even inside an update
+    (parallel TurboFlux ignores the result cap below depth 2)."""
 
+    def __init__(self, w, algo: str, threads: int, cap: int, first: int, budget: float, gated: bool, tag: str):
+        self.algo, self.threads, self.first, self.budget = algo, threads, first, budget
+        self.tmp = Path(tempfile.mkdtemp(prefix=f"csm_ref_{tag}_"))
+        self.out = self.tmp / "rows.csv"
+        self.gate = self.tmp / "gate" if gated else None
+        self.proc = None
+        self.err = None
+        drv = ROOT / "oracle" / "_ref" / "ref_driver"
+        if not drv.exists():
+            self.err = "reference driver not built (oracle/_ref/ref_driver)"
+            return
+        graph = w.directory / (f"data_at_{first}.bin" if first else "data.bin")
+        cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(graph), "-U", str(w.directory / "stream.bin"),
+               "-a", algo, "-t", str(threads), "--first", str(first), "--wall-budget", str(budget),
+               "--out", str(self.out)]
+        if cap:
+            cmd += ["--max-results", str(cap)]
+        if gated:
+            cmd += ["--gate", str(self.gate)]
+        self.t0 = time.perf_counter()
+        self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
 
-def ref_collect(h, hard_timeout: float):
-    """value = updates completed / seconds of incremental matching, plus latency percentiles."""
-    if h is None:
-        return None, "reference driver not built (oracle/_ref/ref_driver)"
-    try:
-        stdout, stderr = h["proc"].communicate(timeout=hard_timeout)
-    except subprocess.TimeoutExpired:
-        h["proc"].kill()
-        return None, f"reference driver did not finish within {hard_timeout:.0f}s"
-    done, elapsed, note = None, None, ""
-    for line in stdout.splitlines():
-        if "updates_done=" in line:
-            kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
-            done, elapsed = int(kv["updates_done"]), float(kv["elapsed_s"])
-            if line.startswith("wall_budget_reached"):
-                note = "(budget reached inside an update)"
-    if done is None:
-        return None, f"reference driver failed (exit {h['proc'].returncode}): {stderr[-300:]}"
-    lat = []
-    if h["out"].exists():
-        for line in h["out"].read_text().splitlines()[1:]:
+    def wait_ready(self, timeout: float) -> bool:
+        if self.proc is None or self.gate is None:
+            return False
+        ready = Path(str(self.gate) + ".ready")
+        t0 = time.perf_counter()
+        while not ready.exists():
+            if self.proc.poll() is not None:
+                self.err = f"reference driver exited ({self.proc.returncode}) before its updates: " + \
+                    self.proc.stderr.read()[-300:]
+                return False
+            if time.perf_counter() - t0 > timeout:
+                self.err = f"reference driver not ready within {timeout:.0f}s"
+                return False
+            time.sleep(0.2)
+        return True
+
+    def go(self) -> None:
+        Path(str(self.gate) + ".go").touch()
+
+    def collect(self, hard_timeout: float) -> dict | None:
+        """updates/s = updates completed / seconds of the update loop, plus latency percentiles."""
+        if self.proc is None:
+            return None
+        try:
+            stdout, stderr = self.proc.communicate(timeout=hard_timeout)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            self.proc.communicate()
+            self.err = f"reference driver did not finish within {hard_timeout:.0f}s"
+            return None
+        done, elapsed, note = None, None, ""
+        for line in stdout.splitlines():
+            if "updates_done=" in line:
+                kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
+                done, elapsed = int(kv["updates_done"]), float(kv["elapsed_s"])
+                if line.startswith("wall_budget_reached"):
+                    note = "(budget reached inside an update)"
+        if done is None:
+            self.err = f"reference driver failed (exit {self.proc.returncode}): {stderr[-300:]}"
+            return None
+        rows = self.rows()
+        lat = rows["latency_ns"].astype(np.float64) if len(rows) else np.zeros(0)
+        if done == 0 or elapsed <= 0:
+            self.err = f"no update finished within {self.budget:.0f}s {note}".strip()
+            return None
+        return {"updates": int(done), "seconds": elapsed, "value": done / elapsed,
+                "first_update": self.first, "last_update": self.first + int(done) - 1,
+                "p50_us": float(np.percentile(lat, 50)) / 1e3 if len(lat) else None,
+                "p99_us": float(np.percentile(lat, 99)) / 1e3 if len(lat) else None,
+                "wall_s": time.perf_counter() - self.t0, "note": note, "algo": self.algo, "threads": self.threads}
+
+    def rows(self) -> np.ndarray:
+        """Per-update rows written so far (stream index, pos, neg, latency)."""
+        dt = np.dtype([("idx", "<i8"), ("pos", "<u8"), ("neg", "<u8"), ("latency_ns", "<u8")])
+        if not self.out.exists():
+            return np.zeros(0, dtype=dt)
+        vals = []
+        for line in self.out.read_text().splitlines()[1:]:
             parts = line.split(",")
             if len(parts) >= 10:
-                lat.append(int(parts[8]))
-    lat = np.array(lat, dtype=np.float64)
-    if done == 0 or elapsed <= 0:
-        return None, f"no update finished within {h['budget']:.0f}s {note}".strip()
-    return {"updates": int(done), "seconds": elapsed, "value": done / elapsed,
-            "p50_ns": float(np.percentile(lat, 50)) if len(lat) else None,
-            "p99_ns": float(np.percentile(lat, 99)) if len(lat) else None,
-            "wall_s": time.perf_counter() - h["t0"], "note": note, "algo": h["algo"], "threads": h["threads"]}, None
+                vals.append((int(parts[0]), int(parts[6]), int(parts[7]), int(parts[8])))
+        return np.array(vals, dtype=dt)
+
+    def kill(self) -> None:
+        if self.proc is not None and self.proc.poll() is None:
+            self.proc.kill()
+            self.proc.communicate()
 
 
-def cpu_lines(w, cfg, budget: float) -> tuple[dict, dict]:
-    """The reference on the host cores: parallel_turboflux on all cores but one (the
-    baseline the targets are stated against) and, on the remaining core, sequential
-    SymBi, which stops at exactly --max-results like the engine does.  Both run at
-    the same time over the same stream prefix."""
+def cpu_line(r: RefRun, res: dict | None, cfg) -> dict:
+    if res is None:
+        return {"value": None, "unit": "updates/s", "cores": r.threads, "kind": "reference", "sample": r.err}
+    return {"value": res["value"], "unit": "updates/s", "cores": res["threads"], "kind": "reference",
+            "updates": res["updates"], "first_update": res["first_update"], "last_update": res["last_update"],
+            "sample": f"stream updates {res['first_update']}..{res['last_update']} ({res['updates']} updates) in "
+                      f"{res['seconds']:.1f}s of incremental matching from the data graph as it stands at update "
+                      f"{res['first_update']}, {res['algo']} -t {res['threads']} (reference sources, sequential "
+                      f"update order, max_results {cfg['max_results']}), {r.budget:.0f}s budget {res['note']}".strip(),
+            "p50_us": res["p50_us"], "p99_us": res["p99_us"]}
+
+
+def start_timed_refs(w, cfg, first: int, budget: float) -> list[RefRun]:
+    """The reference on the host cores from the first timed update: parallel_turboflux on every
+    core (the baseline the targets are stated against), then sequential SymBi on one core, which
+    stops at exactly max_results as the engine does.  Both load at once; their timed loops run
+    one after the other (run_timed_refs)."""
     ncpu = os.cpu_count() or 2
-    ht = ref_start(w, "parallel_turboflux", max(1, ncpu - 1), cfg["max_results"], budget)
-    hs = ref_start(w, "symbi", 1, cfg["max_results"], budget)
+    return [RefRun(w, "parallel_turboflux", ncpu, cfg["max_results"], first, budget, True, "tf"),
+            RefRun(w, "symbi", 1, cfg["max_results"], first, budget, True, "sy")]
+
+
+def run_timed_refs(refs: list[RefRun], cfg, budget: float) -> list[dict]:
     out = []
-    for h in (ht, hs):
-        r, err = ref_collect(h, budget + 900)
-        if r is None:
-            out.append({"value": None, "unit": "updates/s", "cores": h["threads"] if h else 0, "kind": "reference",
-                        "sample": err})
+    for r in refs:
+        res = None
+        if r.wait_ready(3600):
+            r.go()
+            res = r.collect(budget + 600)
         else:
-            out.append({"value": r["value"], "unit": "updates/s", "cores": r["threads"], "kind": "reference",
-                        "sample": f"first {r['updates']} updates of the same stream in {r['seconds']:.1f}s of "
-                                  f"incremental matching, {r['algo']} -t {r['threads']} (reference sources, "
-                                  f"sequential update order), {budget:.0f}s budget {r['note']}".strip(),
-                        "p50_us": (r["p50_ns"] or 0) / 1e3, "p99_us": (r["p99_ns"] or 0) / 1e3})
-    return out[0], out[1]
+            r.kill()
+        out.append(cpu_line(r, res, cfg))
+    return out
+
+
+def parity_check(rows: np.ndarray, gpu: np.ndarray, base: int, cap: int) -> dict:
+    """Per-update pos / neg / capped of the engine (gpu[i] is stream update base + i) against the
+    reference's rows; a reference count at the cap is a capped update (it stops at exactly the cap)."""
+    sel = rows[(rows["idx"] >= base) & (rows["idx"] < base + len(gpu))]
+    if len(sel) == 0:
+        return {"updates_compared": 0, "mismatches": 0}
+    g = gpu[sel["idx"] - base]
+    ref_capped = (sel["pos"] + sel["neg"] >= cap) if cap else np.zeros(len(sel), bool)
+    bad = (g["pos"] != sel["pos"]) | (g["neg"] != sel["neg"]) | ((g["status"] == 1) != ref_capped) | \
+        (g["status"] >= 2)
+    out = {"updates_compared": int(len(sel)), "mismatches": int(bad.sum()), "first_update": int(sel["idx"][0]),
+           "last_update": int(sel["idx"][-1]), "nonzero_updates": int(((sel["pos"] + sel["neg"]) > 0).sum()),
+           "matches": int(sel["pos"].sum() + sel["neg"].sum()), "capped": int(ref_capped.sum())}
+    if bad.any():
+        k = int(np.nonzero(bad)[0][0])
+        out["first_mismatch"] = {"update": int(sel["idx"][k]), "ref": [int(sel["pos"][k]), int(sel["neg"][k])],
+                                 "gpu": [int(g["pos"][k]), int(g["neg"][k]), int(g["status"][k])]}
+    return out
 
 
 def run_reference_arm(args, cfg):
+    """The reference's CPU implementation on this host, on the same workload, config and update
+    range as the GPU arm: parallel_turboflux on every core (value) and sequential SymBi on one
+    core beside it, both from the data graph at the GPU arm's first timed update."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n_updates = max(cfg["min_updates"], (args.warmup + args.steps + 4) * cfg["batch"])
-    w = get_workload(cfg, n_updates)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    n_updates, first = stream_plan(cfg, args.warmup, args.steps, args.e2e_steps)
+    w = get_workload(cfg, n_updates, snapshot_at=first)
     budget = float(os.environ.get("CSM_REF_BUDGET_S", "60"))
-    tf, sy = cpu_lines(w, cfg, budget)
+    tf, sy = run_timed_refs(start_timed_refs(w, cfg, first, budget), cfg, budget)
     line = {"impl": "reference", "metric": METRIC, "unit": "updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "dtype": "u32", "data": "synthetic", "config": {"workload": cfg["workload"]}}
+            "dtype": "u32", "data": "synthetic", "config": bench_config(cfg, args, world)}
     if tf["value"] is None:
         line.update({"value": None, "unavailable": tf["sample"]})
     else:
@@ -374,7 +482,10 @@ def main():
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--plain-sample", type=int, default=3000)
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=30.0,
+                    help="seconds of update loop for each timed reference run")
+    ap.add_argument("--parity-budget", type=float, default=45.0,
+                    help="seconds of update loop for the reference SymBi run the counts are checked against")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the search-shape autotuner")
     ap.add_argument("--tail-enumerate", action="store_true",
@@ -398,7 +509,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from paracosm_b200 import RESULT_DTYPE, Engine
+    from paracosm_b200 import RESULT_DTYPE, Engine, workload
     from paracosm_b200.shard import allreduce_results
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -410,11 +521,19 @@ def main():
     torch.cuda.set_device(local)
     dev = local
     B, W, K, KE = cfg["batch"], args.warmup, args.steps, args.e2e_steps
-    n_updates = max(cfg["min_updates"], (W + max(K, KE)) * B)
-    w = get_workload(cfg, n_updates)
+    n_updates, first = stream_plan(cfg, W, K, KE)
+    w = get_workload(cfg, n_updates, snapshot_at=first)
     qv, qe = w.queries[0]
     stream = w.stream
     assert len(stream) >= (W + max(K, KE)) * B
+
+    # ---- the reference on the host cores (rank 0, one GPU): the timed runs load now and
+    # start their update loops after the GPU legs; the parity run (sequential SymBi from the
+    # initial graph, the warm-up batches' updates) runs meanwhile ----
+    cpu_refs, par_ref = [], None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu_refs = start_timed_refs(w, cfg, first, args.cpu_budget)
+        par_ref = RefRun(w, "symbi", 1, cfg["max_results"], 0, args.parity_budget, False, "parity")
 
     # ---- batched engine, inputs resident in HBM ----
     t0 = time.perf_counter()
@@ -435,18 +554,24 @@ def main():
     d_stream = torch.from_numpy(stream[: (W + K) * B].view(np.uint8).copy()).to(f"cuda:{dev}")
     ext = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{dev}")
     res_dev = torch.empty(K * B * RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{dev}")
-    launches0 = None
+    warm_res = []
     for i in range(W):
-        eng.submit_device(d_stream.data_ptr() + i * B * 16, B)
+        f0 = eng.submit_device(d_stream.data_ptr() + i * B * 16, B)
         eng.wait()
+        warm_res.append(eng.results(f0, B))
+    warm_res = np.concatenate(warm_res) if warm_res else np.zeros(0, dtype=RESULT_DTYPE)
+    if world > 1:
+        t = torch.from_numpy(warm_res.view(np.int64).reshape(-1, 6).copy()).to(f"cuda:{dev}")
+        allreduce_results(t, cap=cfg["max_results"])
+        warm_res = t.cpu().numpy().view(RESULT_DTYPE).reshape(-1)
     st0 = eng.stats()
     launches0 = eng.kernel_launches()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
     with ClockSampler(dev) as clk:
-        ev0.record(ext)
+        evs[0].record(ext)
         for k in range(K):
             eng.submit_device(d_stream.data_ptr() + (W + k) * B * 16, B)
             rp, rn = eng.results_device()
@@ -455,11 +580,12 @@ def main():
                 if world > 1:
                     allreduce_results(view.view(torch.int64).view(-1, 6), cap=cfg["max_results"])
                 res_dev[k * B * RESULT_DTYPE.itemsize:(k + 1) * B * RESULT_DTYPE.itemsize].copy_(view)
-        ev1.record(ext)
-        ev1.synchronize()
+            evs[k + 1].record(ext)
+        evs[K].synchronize()
         eng.wait()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    ms = evs[0].elapsed_time(evs[K])
+    batch_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(K)]
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -494,12 +620,13 @@ def main():
         eng.wait()
     host = torch.from_numpy(stream[W * B:(W + KE) * B].view(np.uint8).copy()).pin_memory()
     e2e_ms = 0.0
+    e2e_same = True
     for k in range(KE):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(ext)
-        first = eng.submit_ptr(host.data_ptr() + k * B * 16, B)
-        r = eng.results(first, B)
+        f0 = eng.submit_ptr(host.data_ptr() + k * B * 16, B)
+        r = eng.results(f0, B)
         if world > 1:
             t = torch.from_numpy(r.view(np.int64).reshape(-1, 6).copy()).to(f"cuda:{dev}")
             allreduce_results(t, cap=cfg["max_results"])
@@ -508,6 +635,9 @@ def main():
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
         assert len(r) == B
+        if k < K:
+            seg = res[k * B:(k + 1) * B]
+            e2e_same &= bool(np.array_equal(r["pos"], seg["pos"]) and np.array_equal(r["neg"], seg["neg"]))
     if world > 1:
         t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -515,39 +645,36 @@ def main():
     e2e_value = KE * B / (e2e_ms / 1e3) if e2e_ms > 0 else None
     eng.close()
 
-    # ---- plain form (one update per launch sequence) on a sample, same initial graph ----
+    # ---- plain form (one update per launch sequence) on the first updates of the timed
+    # window, from the data graph as it stands there: the same updates, in the same graph
+    # state, as the batched form's first timed batch and the reference runs ----
     plain = None
     if rank == 0 and args.plain_sample > 0:
-        P = min(args.plain_sample, len(stream))
-        sample = np.ascontiguousarray(stream[:P])
-        beng = Engine(cfg["algo"], max_results=cfg["max_results"], max_batch=B, device=dev, tail_enumerate=te)
-        beng.set_query(qv, qe)
-        beng.load_graph(w.vlabels, w.edges)
-        beng.build_index()
-        br = beng.run(sample)
-        beng.close()
+        P = min(args.plain_sample, K * B)
+        sample = np.ascontiguousarray(stream[first:first + P])
+        svl, sedges = workload.read_graph(w.directory / f"data_at_{first}.bin")
         forms = {}
         for graphs in (True, False):
-            kw = {k: shape[k] for k in ("warps_per_block", "blocks_per_sm", "donate_every", "split_deep")} if shape else {}
             peng = Engine(cfg["algo"], max_results=cfg["max_results"], mode="plain", device=dev, graphs=graphs,
                           tail_enumerate=te, **kw)
             peng.set_query(qv, qe)
-            peng.load_graph(w.vlabels, w.edges)
+            peng.load_graph(svl, sedges)
             peng.build_index()
             torch.cuda.synchronize()
+            l0 = peng.kernel_launches()
             t1 = time.perf_counter()
             pr = peng.run(sample)
             plain_s = time.perf_counter() - t1
             pst = peng.stats()
-            same = bool(np.array_equal(pr["pos"], br["pos"]) and np.array_equal(pr["neg"], br["neg"]) and
-                        np.array_equal(pr["status"], br["status"]))
+            same = bool(np.array_equal(pr["pos"], res["pos"][:P]) and np.array_equal(pr["neg"], res["neg"][:P]) and
+                        np.array_equal(pr["status"], res["status"][:P]))
             # one submit of P updates, one launch sequence each: an update's service time is the gap
             # between its completion stamp and the previous one's
             svc = np.diff(np.concatenate([[0], np.sort(pr["latency_ns"].astype(np.float64))]))
-            forms[graphs] = {"value": P / plain_s, "updates": P, "device_ms": pst["total_device_ms"],
+            forms[graphs] = {"value": P / plain_s, "updates": P, "first_update": first, "device_ms": pst["total_device_ms"],
                              "p50_us": float(np.percentile(svc, 50)) / 1e3,
                              "p99_us": float(np.percentile(svc, 99)) / 1e3,
-                             "kernel_launches_per_update": pst["kernel_launches"] / P,
+                             "kernel_launches_per_update": (peng.kernel_launches() - l0) / P,
                              "counts_equal_batched": same}
             peng.close()
         plain = dict(forms[True], form="one update per launch sequence, replayed as a CUDA graph")
@@ -559,10 +686,24 @@ def main():
         serving = serve_sweep(w, cfg, [float(r) for r in args.serve_rates.split(",") if r], args.serve_seconds,
                               n_queries=1, device=dev)
 
-    # ---- CPU baseline: the reference compiled from its sources, bounded sample ----
-    cpu, cpu_seq = None, None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, cpu_seq = cpu_lines(w, cfg, args.cpu_budget)
+    # ---- the reference: parity of the counts, then the timed runs one after another ----
+    cpu, cpu_seq, parity, checks = None, None, None, {}
+    if par_ref is not None:
+        par_ref.collect(args.parity_budget + 3600)
+        rows = par_ref.rows()
+        checks = {"from_initial_graph": parity_check(rows, warm_res, 0, cfg["max_results"])}
+        parity = {"reference": "symbi -t 1 (reference sources, sequential update order, cap-honouring)",
+                  "engine": "batched warm-up batches, then the timed window"}
+    if cpu_refs:
+        cpu, cpu_seq = run_timed_refs(cpu_refs, cfg, args.cpu_budget)
+        # the sequential SymBi run times the first updates of the timed window: its counts too
+        checks["timed_window"] = parity_check(cpu_refs[1].rows(), res, first, cfg["max_results"])
+    if parity is not None:
+        parity.update(checks)
+        parity["updates_compared"] = sum(c["updates_compared"] for c in checks.values())
+        parity["mismatches"] = sum(c["mismatches"] for c in checks.values())
+        log(f"parity against the reference SymBi: {parity['updates_compared']} updates, "
+            f"{parity['mismatches']} mismatches")
 
     if rank == 0:
         clocks = clk.summary()
@@ -571,18 +712,16 @@ def main():
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None,
             "dtype": "u32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "plugin": cfg["algo"], "batch": B, "updates_timed": K * B,
-                       "search_shape": shape,
-                       "tail": "enumerated" if te else "counted (independent tail of each order)",
-                       "l2": "inputs larger than L2 (graph ~1.2 GB in HBM)", "max_results": cfg["max_results"],
-                       "parallelism": f"seed-sharded x{world} (replicated graph, one all-reduce per batch)"
-                       if world > 1 else "single GPU"},
+            "config": bench_config(cfg, args, world),
+            "search_shape": shape,
+            "timed_window": {"first_update": first, "last_update": first + K * B - 1, "per_batch_ms": batch_ms},
             "p50_us": float(np.percentile(lat, 50)) / 1e3, "p99_us": float(np.percentile(lat, 99)) / 1e3,
             "plain": plain,
             "batched_over_plain": (value / plain["value"]) if plain else None,
             "serving": serving,
             "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": B * 16,
-                    "d2h_bytes_per_step": B * RESULT_DTYPE.itemsize},
+                    "d2h_bytes_per_step": B * RESULT_DTYPE.itemsize, "first_update": first,
+                    "counts_equal_device_resident": e2e_same},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None,
                          "traffic": SEARCH_DRAM_BYTES_PER_4096 * B / 4096 if cfg["preset"] == "c3" else None,
@@ -591,6 +730,7 @@ def main():
                          "kernel_ms": search_ms, "algorithmic_bytes": work},
             "cpu_baseline": cpu,
             "cpu_baseline_sequential_symbi_capped": cpu_seq,
+            "parity": parity,
             "gpu_launches": launches,
             "clocks": clocks,
             "counts": {"positive": int(res["pos"].sum()), "negative": int(res["neg"].sum()),

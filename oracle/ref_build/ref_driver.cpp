@@ -104,8 +104,10 @@ class EnumHashBuf : public std::streambuf {
 
 struct Args {
   std::string q, d, u, algo = "graphflow", out, dbin, ubin, dump_index;
+  std::string gate;         // after preprocessing: create <gate>.ready, start once <gate>.go exists
   std::vector<long> dump_at;  // update counts after which the index is dumped (0: after preprocessing)
   size_t threads = 1, auto_tuning = 0, max_updates = SIZE_MAX;
+  size_t first = 0;         // index of the first stream update to run (the data graph is the state there)
   uint64_t max_results = UINT32_MAX;
   double time_budget = 0;   // stop after the update that crosses this many seconds
   double wall_budget = 0;   // hard limit: report and exit even inside an update
@@ -163,6 +165,8 @@ void usage() {
           "ref_driver -q query -d data|-D data.bin -u stream|-U stream.bin -a algo\n"
           "  [-t threads] [--auto-tuning 0|1] [--max-results N] [--homo 0|1]\n"
           "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S] [--wall-budget S]\n"
+          "  [--first N]   (start at stream update N; give the data graph as it stands there)\n"
+          "  [--gate PATH] (after preprocessing write PATH.ready; start the updates once PATH.go exists)\n"
           "  [--dump-index FILE --dump-at N,N,...]   (symbi / turboflux: root, DAG, d1 / d2 flags)\n");
 }
 
@@ -186,6 +190,8 @@ int main(int argc, char** argv) {
     else if (k == "--hash") a.hash = true;
     else if (k == "--out") a.out = nxt();
     else if (k == "--max-updates") a.max_updates = std::stoull(nxt());
+    else if (k == "--first") a.first = std::stoull(nxt());
+    else if (k == "--gate") a.gate = nxt();
     else if (k == "--time-budget") a.time_budget = std::stod(nxt());
     else if (k == "--wall-budget") a.wall_budget = std::stod(nxt());
     else if (k == "--dump-index") a.dump_index = nxt();
@@ -225,7 +231,11 @@ int main(int argc, char** argv) {
 
   if (!a.ubin.empty()) { if (!read_binary_stream(a.ubin, data)) { fprintf(stderr, "bad stream %s\n", a.ubin.c_str()); return 1; } }
   else data.LoadUpdateStream(a.u);
-  size_t n_up = std::min(data.updates_vec_.size(), a.max_updates);
+  // --first N: the data graph given is the state after updates [0, N), and the
+  // loop runs updates N, N + 1, ... in order (rows keep their stream index)
+  const size_t first = std::min(a.first, data.updates_vec_.size());
+  size_t n_up = data.updates_vec_.size() - first;
+  if (a.max_updates < n_up) n_up = a.max_updates;
 
   FILE* fo = nullptr;
   if (!a.out.empty()) {
@@ -243,6 +253,22 @@ int main(int argc, char** argv) {
     fprintf(stderr, "--dump-index supports symbi and turboflux\n");
     return 2;
   }
+  if (!a.gate.empty()) {
+    // Several runs can load and preprocess at the same time while their timed
+    // update loops are started one after another by whoever holds the gate.
+    FILE* fr = fopen((a.gate + ".ready").c_str(), "w");
+    if (!fr) { fprintf(stderr, "cannot write %s.ready\n", a.gate.c_str()); return 1; }
+    fclose(fr);
+    const std::string go = a.gate + ".go";
+    auto g0 = std::chrono::steady_clock::now();
+    while (access(go.c_str(), F_OK) != 0) {
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - g0).count() > 7200.0) {
+        fprintf(stderr, "gate %s not opened within 7200 s\n", go.c_str());
+        return 1;
+      }
+      std::this_thread::sleep_for(std::chrono::milliseconds(20));
+    }
+  }
   if (a.hash) old = std::cout.rdbuf(&hb);
 
   size_t pos_last = 0, neg_last = 0, unsafe = 0, nv = 0, ne = 0, done = 0;
@@ -251,16 +277,16 @@ int main(int argc, char** argv) {
   if (a.wall_budget > 0) {
     // Some reference plugins ignore the result cap inside their parallel
     // search, so one update can run for hours: report what finished and exit.
-    std::thread([ts, &a]() {
+    std::thread([ts, &a, first]() {
       std::this_thread::sleep_for(std::chrono::duration<double>(a.wall_budget));
       double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
-      printf("wall_budget_reached updates_done=%zu elapsed_s=%.6f\n", g_done.load(), el);
+      printf("wall_budget_reached updates_done=%zu elapsed_s=%.6f first=%zu\n", g_done.load(), el, first);
       fflush(stdout);
       _exit(0);
     }).detach();
   }
   for (size_t i = 0; i < n_up; i++) {
-    const InsertUnit& up = data.updates_vec_[i];
+    const InsertUnit& up = data.updates_vec_[first + i];
     auto s = std::chrono::steady_clock::now();
     if (up.type == 'v' && up.is_add) { mm->AddVertex(up.id1, up.label); nv++; }
     else if (up.type == 'v') { mm->RemoveVertex(up.id1); nv++; }
@@ -272,7 +298,7 @@ int main(int argc, char** argv) {
     mm->GetNumPositiveResults(pc);
     mm->GetNumNegativeResults(nc);
     uint64_t h = a.hash ? hb.take() : 0;
-    if (fo) fprintf(fo, "%zu,%c,%d,%u,%u,%u,%zu,%zu,%llu,%llu\n", i, up.type, (int)up.is_add, up.id1,
+    if (fo) fprintf(fo, "%zu,%c,%d,%u,%u,%u,%zu,%zu,%llu,%llu\n", first + i, up.type, (int)up.is_add, up.id1,
                     up.id2, up.label, pc - pos_last, nc - neg_last, (unsigned long long)lat[i],
                     (unsigned long long)h);
     if (fo) fflush(fo);  // completed updates survive a kill of a run that hangs on a later one
@@ -303,8 +329,8 @@ int main(int argc, char** argv) {
   printf("Incremental Matching: %.3f ms\n", inc_s * 1e3);
   printf("%zu vertex updates.\n%zu edge updates.\n%zu unsafe updates.\n", nv, ne, unsafe);
   printf("%zu positive matches.\n%zu negative matches.\n", pos_last, neg_last);
-  printf("updates_done=%zu elapsed_s=%.6f updates_per_s=%.3f p50_ns=%llu p99_ns=%llu threads=%zu\n", done, inc_s,
-         done / std::max(inc_s, 1e-12), pct(0.50), pct(0.99), a.threads);
+  printf("updates_done=%zu elapsed_s=%.6f updates_per_s=%.3f p50_ns=%llu p99_ns=%llu threads=%zu first=%zu\n", done,
+         inc_s, done / std::max(inc_s, 1e-12), pct(0.50), pct(0.99), a.threads, first);
   fflush(stdout);
   // Skip destructors of the large hash maps: exit directly.
   _exit(0);

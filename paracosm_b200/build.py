@@ -27,7 +27,24 @@ HOST = PKG / "host"
 LIB = PKG / "_lib"
 BIN = PKG / "_bin"
 OBJ = PKG / "_lib" / "obj"
-REF_SRC = Path("/root/reference/ParaCOSM/CSM")
+
+
+def reference_sources() -> Path | None:
+    """ParaCOSM/CSM of the reference checkout, when it is present: $PARACOSM_REFERENCE
+    (the checkout root), else BASELINE.json's reference_path.  The reference is
+    only compiled as the checker and CPU baseline (oracle/_ref)."""
+    import json
+
+    root = os.environ.get("PARACOSM_REFERENCE")
+    if not root:
+        try:
+            root = json.loads((ROOT / "BASELINE.json").read_text()).get("reference_path")
+        except (OSError, ValueError):
+            root = None
+    if not root:
+        return None
+    src = Path(root) / "ParaCOSM" / "CSM"
+    return src if src.exists() else None
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
@@ -102,8 +119,9 @@ def build_host(force: bool = False) -> None:
 def build_oracle(force: bool = False) -> None:
     env = dict(os.environ, CXX=CXX)
     _run(["make", "-C", str(ROOT / "oracle")] + (["-B"] if force else []), cwd=ROOT)
-    if REF_SRC.exists():
-        _run(["make", "-C", str(ROOT / "oracle" / "ref_build"), f"REF={REF_SRC}", "-j8"], cwd=ROOT)
+    ref = reference_sources()
+    if ref is not None:
+        _run(["make", "-C", str(ROOT / "oracle" / "ref_build"), f"REF={ref}", "-j8"], cwd=ROOT)
     del env
 
 

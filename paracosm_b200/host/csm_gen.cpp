@@ -3,11 +3,14 @@
 //
 //   csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--calig] [--no-binary]
 //           [--log2-n K] [--avg-degree D] [--vlabels L] [--zipf S] [--elabels L]
-//           [--updates N] [--insert-frac F] [--holdout-frac F]
+//           [--updates N] [--insert-frac F] [--holdout-frac F] [--snapshot-at N]
 //           [--query SIZE:dense|sparse[:EXTRA[:MINDEG]]] (repeatable; replaces the preset's)
 //
 // DIR receives data.bin / stream.bin (binary), data.graph / stream.txt (text,
-// with --text), query_<i>.graph, and meta.txt (the spec and sizes).  --calig
+// with --text), query_<i>.graph, and meta.txt (the spec and sizes).
+// --snapshot-at N also writes data_at_<N>.bin: the data graph left by the
+// first N updates of the stream, from which a run can start at update N
+// (binary only).  --calig
 // also writes data.calig / stream.calig / query_<i>.calig in the reference
 // CaLiG program's formats (no edge labels; deletions as negative ids).
 #include <sys/stat.h>
@@ -28,7 +31,7 @@ static void usage() {
   fprintf(stderr,
           "csm_gen --preset c1|c2|c3|c4|c5 --out DIR [--seed S] [--text] [--calig] [--no-binary]\n"
           "        [--log2-n K] [--avg-degree D] [--vlabels L] [--zipf S] [--elabels L]\n"
-          "        [--updates N] [--insert-frac F] [--holdout-frac F]\n"
+          "        [--updates N] [--insert-frac F] [--holdout-frac F] [--snapshot-at N]\n"
           "        [--query SIZE:dense|sparse[:EXTRA[:MINDEG]]]...\n");
 }
 
@@ -55,6 +58,7 @@ int main(int argc, char** argv) {
       else if (k == "--updates") s.n_updates = std::stoull(nxt());
       else if (k == "--insert-frac") s.insert_fraction = std::stod(nxt());
       else if (k == "--holdout-frac") s.holdout_fraction = std::stod(nxt());
+      else if (k == "--snapshot-at") s.snapshot_at = std::stoull(nxt());
       else if (k == "--query") {
         if (!queries_set) { s.queries.clear(); queries_set = true; }
         std::string v = nxt();
@@ -84,6 +88,8 @@ int main(int argc, char** argv) {
     ok &= save_graph_binary(out + "/data.bin", w.initial);
     ok &= save_stream_binary(out + "/stream.bin", w.stream);
   }
+  if (s.snapshot_at)
+    ok &= save_graph_binary(out + "/data_at_" + std::to_string(s.snapshot_at) + ".bin", w.snapshot);
   if (text) {
     ok &= save_graph_text(out + "/data.graph", w.initial);
     ok &= save_stream_text(out + "/stream.txt", w.stream);

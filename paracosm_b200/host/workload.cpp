@@ -300,7 +300,18 @@ bool generate(const WorkloadSpec& s, Workload& w, std::string& err) {
   std::shuffle(kinds.begin(), kinds.end(), sr);
   uint64_t next_ins = 0;
   w.stream.reserve(s.n_updates);
+  auto take_snapshot = [&]() {
+    w.snapshot.n = n; w.snapshot.n_vlabels = s.n_vlabels; w.snapshot.n_elabels = s.n_elabels;
+    w.snapshot.vlabels = all.vlabels;
+    std::vector<uint64_t> ids(cur);
+    std::sort(ids.begin(), ids.end());
+    w.snapshot.edges.resize(3 * ids.size());
+    for (size_t k = 0; k < ids.size(); k++)
+      for (int c = 0; c < 3; c++) w.snapshot.edges[3 * k + c] = all.edges[3 * ids[k] + c];
+  };
+  if (s.snapshot_at > s.n_updates) { err = "snapshot position beyond the stream"; return false; }
   for (uint64_t i = 0; i < s.n_updates; i++) {
+    if (s.snapshot_at && i == s.snapshot_at) take_snapshot();
     Update u{};
     u.type = 'e';
     if (kinds[i]) {
@@ -315,6 +326,7 @@ bool generate(const WorkloadSpec& s, Workload& w, std::string& err) {
     }
     w.stream.push_back(u);
   }
+  if (s.snapshot_at && s.snapshot_at == s.n_updates) take_snapshot();
   (void)n_del;
 
   // queries sampled from the initial graph

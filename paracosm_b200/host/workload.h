@@ -37,6 +37,9 @@ struct WorkloadSpec {
   uint64_t n_updates = 2000;
   double insert_fraction = 1.0;
   double holdout_fraction = 0.0;   // if > 0: held-out = fraction * E (else = #inserts)
+  // > 0: also keep the data graph as it stands after the first snapshot_at
+  // updates of the stream (Workload::snapshot), so that a run can start there
+  uint64_t snapshot_at = 0;
 };
 
 struct Query {
@@ -52,6 +55,7 @@ struct Workload {
   std::vector<Update> stream;
   std::vector<Query> queries;
   uint64_t total_edges = 0;        // unique edges generated before the hold-out
+  EdgeList snapshot;               // graph after stream[0 .. spec.snapshot_at) (when snapshot_at > 0)
 };
 
 // Presets for the named workloads ("c1".."c5"); returns false for an unknown name.

@@ -20,7 +20,36 @@ def pytest_configure(config):
 
 
 def golden_cases() -> list[str]:
-    return sorted(d.name for d in GOLDEN.iterdir() if d.is_dir() and (d / "expected.csv").exists())
+    """Fixtures that store their inputs in the reference's text formats."""
+    return sorted(d.name for d in GOLDEN.iterdir()
+                  if d.is_dir() and (d / "expected.csv").exists() and (d / "data.graph").exists())
+
+
+def load_c3_shape(out_dir: Path) -> dict:
+    """The c3_shape case: its inputs rebuilt by the seeded generator (checked against the
+    SHA-256 recorded with the fixture) and the reference SymBi's per-update counts, as full
+    arrays over the stream (updates not listed in expected.csv count 0)."""
+    import hashlib
+    import subprocess
+
+    from paracosm_b200 import workload
+    d = GOLDEN / "c3_shape"
+    params = json.loads((d / "params.json").read_text())
+    if not (out_dir / "stream.bin").exists():
+        subprocess.run([str(ROOT / "paracosm_b200" / "_bin" / "csm_gen")] + params["generator"] +
+                       ["--out", str(out_dir)], check=True, capture_output=True)
+    for f, h in params["sha256"].items():
+        got = hashlib.sha256((out_dir / f).read_bytes()).hexdigest()
+        assert got == h, f"the generator no longer writes the c3_shape inputs: {f} differs"
+    w = workload.load(out_dir)
+    n = params["updates"]
+    assert len(w.stream) == n
+    exp = {k: np.zeros(n, dtype=np.uint64) for k in ("pos", "neg", "hash", "cap_pos", "cap_neg")}
+    for r in csv.DictReader(open(d / "expected.csv")):
+        i = int(r["idx"])
+        exp["pos"][i], exp["neg"][i], exp["hash"][i] = int(r["symbi_pos"]), int(r["symbi_neg"]), int(r["symbi_hash"])
+        exp["cap_pos"][i], exp["cap_neg"][i] = int(r["symbi_cap_pos"]), int(r["symbi_cap_neg"])
+    return {"w": w, "params": params, "exp": exp}
 
 
 def calig_cases() -> list[str]:

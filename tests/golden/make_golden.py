@@ -18,6 +18,17 @@ before the stream.
     python tests/golden/make_golden.py --index  # only the index fixtures
     python tests/golden/make_golden.py --initial  # only initial.json (InitialMatching counts of csm)
     python tests/golden/make_golden.py --calig    # only the calig_* cases
+    python tests/golden/make_golden.py --c3shape  # only the c3_shape case
+
+The c3_shape case has the shape of the 2^22-vertex SymBi benchmark at a size
+the CPU finishes: 2^16 vertices, average degree 28, 16 vertex labels
+Zipf(1.2), 4 edge labels, a 16-vertex dense query (average degree >= 4), an
+80/20 insert/delete stream of 70,000 updates.  Its inputs are not stored: the
+seeded generator rebuilds them, and params.json holds the SHA-256 of the
+files it writes so that a changed generator is caught.  expected.csv lists
+only the updates where some count is nonzero (every other update counts 0):
+sequential SymBi's pos / neg / match-set hash with max_results 1e6, and its
+pos / neg with max_results 20,000 (it stops at exactly the cap).
 
 The calig_* cases are in the reference CaLiG program's own formats (data,
 query, stream; no edge labels, insertions only, since the reference cannot
@@ -146,7 +157,49 @@ def write_initial(d: Path, homo: bool) -> None:
     (d / "initial.json").write_text(json.dumps(out) + "\n")
 
 
+C3_SHAPE = ["--preset", "c3", "--log2-n", "16", "--updates", "70000", "--seed", "35"]
+C3_SHAPE_CAPS = (1_000_000, 20_000)
+
+
+def c3_shape_files(out: Path) -> dict:
+    """Generates the c3_shape inputs into `out`; returns the SHA-256 of each file."""
+    import hashlib
+
+    subprocess.run([str(GEN)] + C3_SHAPE + ["--out", str(out)], check=True, capture_output=True)
+    return {f: hashlib.sha256((out / f).read_bytes()).hexdigest()
+            for f in ("data.bin", "stream.bin", "query_0.graph")}
+
+
+def write_c3_shape() -> None:
+    d = HERE / "c3_shape"
+    tmp = HERE / "_tmp_c3_shape"
+    if tmp.exists():
+        shutil.rmtree(tmp)
+    sha = c3_shape_files(tmp)
+    full, _ = pyoracle.ref_run(tmp / "query_0.graph", tmp / "data.bin", tmp / "stream.bin", "symbi",
+                               max_results=C3_SHAPE_CAPS[0], want_hash=True, binary=True, timeout=3600)
+    capped, _ = pyoracle.ref_run(tmp / "query_0.graph", tmp / "data.bin", tmp / "stream.bin", "symbi",
+                                 max_results=C3_SHAPE_CAPS[1], binary=True, timeout=3600)
+    shutil.rmtree(tmp)
+    d.mkdir(exist_ok=True)
+    n = len(full)
+    with open(d / "expected.csv", "w") as f:
+        f.write("idx,symbi_pos,symbi_neg,symbi_hash,symbi_cap_pos,symbi_cap_neg\n")
+        for i in range(n):
+            a, c = full[i], capped[i]
+            if a["pos"] or a["neg"] or c["pos"] or c["neg"]:
+                f.write(f"{i},{a['pos']},{a['neg']},{a['hash']},{c['pos']},{c['neg']}\n")
+    (d / "params.json").write_text(json.dumps({
+        "generator": C3_SHAPE, "updates": n, "max_results": C3_SHAPE_CAPS[0], "max_results_capped": C3_SHAPE_CAPS[1],
+        "sha256": sha, "reference": "ParaCOSM/CSM/matching/SymBi (sequential), SingleThreadUpdate order"},
+        indent=1) + "\n")
+    print("c3_shape updates", n, "nonzero", sum(1 for i in range(n) if full[i]["pos"] or full[i]["neg"]))
+
+
 def main() -> None:
+    if "--c3shape" in sys.argv:
+        write_c3_shape()
+        return
     if "--calig" in sys.argv:
         for name, args in CALIG_CASES.items():
             write_calig(name, args)

@@ -229,3 +229,20 @@ def test_group_assignments_equal_brute_force():
         anyway = int(np.prod([len(s) for s in sets]))
         assert pyoracle.group_assignments(g, classes) == inj, (sets, classes)
         assert pyoracle.group_assignments(g, classes, homo=True) == anyway
+
+
+def test_oracle_matches_reference_symbi_on_the_c3_shape(tmp_path_factory):
+    """The C3 shape (16-vertex dense query, 16 Zipf vertex labels, 4 edge labels) at 2^16
+    vertices: the oracle's counts and match-set hashes equal the reference SymBi's on the first
+    13,000 updates (six of them nonzero, deletions among them; the rest of the 70,000-update
+    stream is checked on the GPU against the same fixture)."""
+    from conftest import load_c3_shape
+    c = load_c3_shape(tmp_path_factory.mktemp("c3_shape"))
+    w, x = c["w"], c["exp"]
+    qv, qe = w.queries[0]
+    n = 13_000
+    ref = pyoracle.run(qv, qe, w.vlabels, w.edges, w.stream[:n], max_results=c["params"]["max_results"])
+    assert np.array_equal(ref["pos"], x["pos"][:n])
+    assert np.array_equal(ref["neg"], x["neg"][:n])
+    assert np.array_equal(ref["hash"], x["hash"][:n])
+    assert int(((x["pos"][:n] + x["neg"][:n]) > 0).sum()) == 6
