@@ -233,7 +233,14 @@ int csm_gpu_submit_device(csm_ctx* ctx, uint64_t n, const csm_update* d_ups);
  * contain the edge in the context's current graph -- the count an insertion
  * of an edge already in the graph reports -- into d_counts[i] (device
  * memory, capped at max_results; 0 for an edge with an unknown endpoint).
- * The graph is not modified.  This entry point has no counterpart in the
+ * For the CaLiG-style plugin that count is 0: its rule for an insertion of
+ * a present edge.  An edge that is not in the graph is searched as the
+ * anchor all the same, against the current candidate index (exact for
+ * GraphFlow; for the index plugins the insertion itself may add candidates
+ * that this count misses).  The probe counts the whole graph (a seed-sharded
+ * context's shard settings and the per-update deadline do not apply), and on
+ * an attached query it reads the owner's graph after the owner's last
+ * submit.  The graph is not modified.  This entry point has no counterpart in the
  * reference.  It is for callers that cannot allocate device memory where
  * they need counts (a locked or stream-ordered memory pool, a latency-
  * critical loop in which an allocation would synchronise the device): it

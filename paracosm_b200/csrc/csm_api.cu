@@ -1736,11 +1736,18 @@ struct CtxView {
   uint64_t cap;
   int homo, want_hash;
   uint32_t warps, bps;
+  uint32_t dup_zero;       // CaLiG: an insertion of a present edge counts 0
+  cudaEvent_t owner_end;   // attached query: end of the owner's last submit (null otherwise)
 };
 
 bool ctx_view(csm_ctx* ctx, CtxView* v) {
   if (!ctx || !v || !ctx->has_graph || !ctx->has_plan) return false;
-  v->g = ctx->g;
+  if (ctx->owner && !ctx->owner->has_graph) return false;
+  // an attached query reads its owner's graph, which the owner's submits
+  // mutate on the owner's stream
+  v->g = ctx->owner ? ctx->owner->g : ctx->g;
+  v->owner_end = ctx->owner ? ctx->owner->ev_end : nullptr;
+  v->dup_zero = ctx->cfg.algorithm == CSM_ALGO_CALIG ? 1u : 0u;
   v->plan = ctx->d_plan;
   v->d2 = ctx->index.d2;
   v->d2_words = ctx->index.words;
@@ -1752,13 +1759,12 @@ bool ctx_view(csm_ctx* ctx, CtxView* v) {
   v->cap = ctx->cfg.max_results;
   v->homo = ctx->cfg.homomorphism;
   v->want_hash = ctx->cfg.want_hash;
+  // the launch shape of the submit path's enumerating search (the probe does
+  // not count tails)
   uint32_t warps = ctx->cfg.warps_per_block ? ctx->cfg.warps_per_block : 8;
   if (warps != 4 && warps != 8 && warps != 16) warps = 8;
   uint32_t bps = ctx->cfg.blocks_per_sm;
-  if (!bps) {
-    const size_t smem = search_smem_bytes(ctx->nq, warps);
-    bps = (uint32_t)std::max<size_t>(1, std::min<size_t>(64 / warps, (200 * 1024) / std::max<size_t>(smem, 1)));
-  }
+  if (!bps) bps = std::max<uint32_t>(1, search_max_blocks(ctx->nq, warps, 0));
   v->warps = warps;
   v->bps = bps;
   return true;

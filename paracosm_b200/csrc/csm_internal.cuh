@@ -135,6 +135,17 @@ __device__ __forceinline__ bool contains_u32(const uint32_t* a, uint64_t lo, uin
   return p < hi && a[p] == x;
 }
 
+// Finds edge (x, y) in the union graph; returns its folded label or kNone.
+__device__ __forceinline__ uint32_t find_label(const DevGraph& g, const uint32_t* pool, uint32_t x, uint32_t y) {
+  const uint32_t ly = g.vlabel[y];
+  for (uint32_t l = 0; l < g.n_el; l++) {
+    uint64_t lo, hi;
+    segment(g, x, ly * g.n_el + l, lo, hi);
+    if (contains_u32(pool, lo, hi, y)) return l;
+  }
+  return kNone;
+}
+
 // Is edge (v, w) with combo c present at batch time t?  Only called for
 // edges found in the union graph; edges not touched in this batch are present.
 __device__ __forceinline__ bool present_at(const DevGraph& g, uint32_t v, uint32_t c, uint32_t w, int32_t t) {

@@ -134,17 +134,6 @@ __global__ void k_batch_init(const csm_update* ups, uint32_t B, DevGraph g, uint
   info[s] = inf;
 }
 
-// Finds edge (x, y) in the union graph; returns its label or kNone.
-__device__ uint32_t find_label(const DevGraph& g, const uint32_t* pool, uint32_t x, uint32_t y) {
-  const uint32_t ly = g.vlabel[y];
-  for (uint32_t l = 0; l < g.n_el; l++) {
-    uint64_t lo, hi;
-    segment(g, x, ly * g.n_el + l, lo, hi);
-    if (contains_u32(pool, lo, hi, y)) return l;
-  }
-  return kNone;
-}
-
 __device__ __forceinline__ void emit2(uint64_t* key, unsigned int* n, uint32_t cap, uint64_t k1, uint64_t k2,
                                       uint64_t* val, uint64_t v, unsigned int* err) {
   unsigned int i = atomicAdd(n, 2u);

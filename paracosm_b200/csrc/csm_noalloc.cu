@@ -34,6 +34,8 @@ struct CtxView {
   uint64_t cap;
   int homo, want_hash;
   uint32_t warps, bps;
+  uint32_t dup_zero;       // CaLiG: an insertion of a present edge counts 0
+  cudaEvent_t owner_end;   // attached query: end of the owner's last submit (null otherwise)
 };
 bool ctx_view(csm_ctx* ctx, CtxView* v);  // csm_api.cu
 
@@ -86,6 +88,9 @@ __global__ void k_probe_prep(const csm_update* edges, uint32_t n, DevGraph g, Up
   const bool ok = u.type == 'e' && u.id1 < g.n && u.id2 < g.n && u.id1 != u.id2 && g.vlabel[u.id1] != kNone &&
                   g.vlabel[u.id2] != kNone;
   inf.flags = ok ? (UF_VALID | UF_ADD) : UF_INVALID;
+  // an edge already in the graph is a duplicate insertion (what the submit
+  // path's k_resolve marks): the CaLiG rule counts it 0
+  if (ok && find_label(g, g.pools[g.ps->active], u.id1, u.id2) != kNone) inf.flags |= UF_DUP;
   info[i] = inf;
   count[i] = 0; hash[i] = 0; bytes[i] = 0; stop[i] = 0;
 }
@@ -155,9 +160,15 @@ extern "C" int csm_gpu_probe_noalloc(csm_ctx* ctx, uint32_t n, const csm_update*
 
   const uint32_t task_cap = n * 2 * v.n_anchor;
   const uint32_t nb = (n + 255) / 256;
+  if (v.owner_end) {
+    // an attached query's graph is mutated by its owner's submits, on the
+    // owner's stream: read it after the owner's last submit
+    e = cudaStreamWaitEvent(v.st, v.owner_end, 0);
+    if (e != cudaSuccess) return set_err(CSM_ECUDA, "probe: wait for the owner: %s", cudaGetErrorString(e));
+  }
   k_probe_prep<<<nb, 256, 0, v.st>>>(d_edges, n, v.g, info, count, hash, bytes, stop, words, sstat);
   k_seed<<<(n + 127) / 128, 128, 0, v.st>>>(n, info, v.g, v.plan, v.d2, v.d2_words, tasks, words + 0, task_cap, safe,
-                                             words + 2);
+                                             words + 2, 0, 1, 0, v.dup_zero);
   SearchParams sp{};
   sp.g = v.g; sp.plan = v.plan; sp.tasks = tasks; sp.n_tasks = words + 0; sp.task_cap = task_cap;
   sp.task_next = words + 1; sp.info = info; sp.count = count; sp.hash = hash; sp.bytes = bytes; sp.stop = stop;

@@ -92,69 +92,123 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
   return v;
 }
 
+// Bounds of up to four back segments of one position for one prefix, with
+// the batch touch count of each row (0: the row holds no entry inserted or
+// deleted in this batch, so every entry of it is present at every batch time).
+struct SegQuad {
+  uint32_t v[4], c[4], lo[4], hi[4], tc[4];
+};
+
+// Loads back entries b0 .. b0 + 3 of position P for prefix m: all loads are
+// independent, so the quad costs one round trip to L2.  The bounds of entry
+// `skip` are not loaded (the driver: the candidate came from it), but its
+// touch count is (its edge still needs the batch-time presence test).
+__device__ __forceinline__ void load_quad(const DevGraph& g, const PlanAnchor* A, const PlanPos& P, uint32_t b0,
+                                          const uint32_t* m, uint32_t skip, SegQuad& s) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const uint32_t b = b0 + (uint32_t)i;
+    s.v[i] = 0; s.c[i] = 0; s.lo[i] = 0; s.hi[i] = 0; s.tc[i] = 0;
+    if (b < P.nb) {
+      s.v[i] = m[A->back_pos[P.boff + b]];
+      s.c[i] = A->back_combo[P.boff + b];
+      if (b != skip) {
+        const uint32_t* d = g.dir + (size_t)s.v[i] * (g.nc + 1) + s.c[i];
+        const uint32_t base = (uint32_t)g.row_off[s.v[i]];
+        s.lo[i] = base + d[0];
+        s.hi[i] = base + d[1];
+      }
+      s.tc[i] = g.t_count[s.v[i]];
+    }
+  }
+}
+
+// Is x in each loaded segment of the quad (every entry but `skip`), and is
+// every back edge of the quad present at batch time t?  The lower-bound
+// searches of the four segments advance in lockstep (one round trip per
+// round); a probe that lands on x ends that search, so no separate load
+// confirms the final position (if x is in the segment, the search must probe
+// its slot before it can end there).
+__device__ __forceinline__ bool quad_joins(const DevGraph& g, const uint32_t* pool, const PlanPos& P, uint32_t b0,
+                                           uint32_t skip, uint32_t x, int32_t t, SegQuad& s) {
+  uint32_t need = 0, found = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const uint32_t b = b0 + (uint32_t)i;
+    if (b < P.nb && b != skip) need |= 1u << i;
+  }
+  for (;;) {
+    bool more = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (s.lo[i] < s.hi[i]) {
+        const uint32_t mid = (s.lo[i] + s.hi[i]) >> 1;
+        const uint32_t val = pool[mid];
+        if (val < x) s.lo[i] = mid + 1;
+        else if (val > x) s.hi[i] = mid;
+        else { found |= 1u << i; s.hi[i] = s.lo[i]; }
+        more = true;
+      }
+    }
+    if (!more) break;
+  }
+  if ((found & need) != need) return false;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    if (b0 + (uint32_t)i >= P.nb || s.tc[i] == 0) continue;
+    if (!present_at(g, s.v[i], s.c[i], x, t)) return false;
+  }
+  return true;
+}
+
 // Full candidate check of data vertex x for position `pos` given the matched
-// prefix m[0 .. pos-1]; `dsel` is the back entry whose segment produced x.
-// The joins are done four back entries at a time: their segment bounds are
-// loaded together and their binary searches advance in lockstep, so each
-// round trip to L2 serves up to four searches instead of one.
+// prefix m[0 .. pos-1]; `dsel` is the back entry whose segment produced x and
+// q0 the first quad of pos's back entries, already loaded (load_quad with
+// skip = dsel).  The candidate-filter word is loaded before the first join
+// round and tested after it, so the two round trips overlap.
+__device__ __forceinline__ bool check_candidate_q(const SearchParams& p, const uint32_t* pool, const PlanAnchor* A,
+                                                  uint32_t pos, uint32_t x, const uint32_t* m, uint32_t dsel,
+                                                  int32_t t, SegQuad& q0, uint32_t lab_mask = 0xffffffffu) {
+  const PlanPos P = A->pos[pos];
+  const uint64_t fw = p.d2 ? p.d2[(uint64_t)P.qv * p.d2_words + (x >> 6)] : ~0ULL;
+  bool ok = true;
+  if (!p.homo) {
+    for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) ok &= m[__ffs(mk) - 1] != x;
+  }
+  if (!ok) return false;
+  ok = quad_joins(p.g, pool, P, 0, dsel, x, t, q0);
+  if (!((fw >> (x & 63)) & 1ULL)) return false;
+  if (!ok) return false;
+  for (uint32_t b0 = 4; b0 < P.nb; b0 += 4) {
+    SegQuad q;
+    load_quad(p.g, A, P, b0, m, dsel, q);
+    if (!quad_joins(p.g, pool, P, b0, dsel, x, t, q)) return false;
+  }
+  return true;
+}
+
+// The same check when no quad was prefetched.
 __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uint32_t* pool, const PlanAnchor* A,
                                                 uint32_t pos, uint32_t x, const uint32_t* m, uint32_t dsel,
                                                 int32_t t, uint32_t lab_mask = 0xffffffffu) {
-  const PlanPos P = A->pos[pos];
-  if (!p.homo) {
-    for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) {
-      if (m[__ffs(mk) - 1] == x) return false;
-    }
-  }
-  if (p.d2 && !d2_bit(p.d2, p.d2_words, P.qv, x)) return false;
-  for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
-    uint32_t v[4], c[4], lo[4], hi[4], end[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const uint32_t b = b0 + (uint32_t)i;
-      v[i] = 0; c[i] = 0; lo[i] = 0; hi[i] = 0; end[i] = 0;
-      if (b < P.nb) {
-        v[i] = m[A->back_pos[P.boff + b]];
-        c[i] = A->back_combo[P.boff + b];
-        if (b != dsel) {
-          uint64_t l, h;
-          segment(p.g, v[i], c[i], l, h);
-          lo[i] = (uint32_t)l; hi[i] = (uint32_t)h; end[i] = (uint32_t)h;
-        }
-      }
-    }
-    // lower_bound of x in each segment, one probe per segment per round
-    for (;;) {
-      bool more = false;
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        if (lo[i] < hi[i]) {
-          const uint32_t mid = (lo[i] + hi[i]) >> 1;
-          if (pool[mid] < x) lo[i] = mid + 1; else hi[i] = mid;
-          more = true;
-        }
-      }
-      if (!more) break;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const uint32_t b = b0 + (uint32_t)i;
-      if (b >= P.nb || b == dsel) continue;
-      if (lo[i] >= end[i] || pool[lo[i]] != x) return false;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      if (b0 + (uint32_t)i >= P.nb) continue;
-      if (!present_at(p.g, v[i], c[i], x, t)) return false;
-    }
-  }
-  return true;
+  SegQuad q0;
+  load_quad(p.g, A, A->pos[pos], 0, m, dsel, q0);
+  return check_candidate_q(p, pool, A, pos, x, m, dsel, t, q0, lab_mask);
+}
+
+// Number of entries of segment (v, c) = [lo, hi) present at batch time t,
+// given the row's touch count tc (seg_size_at with the count already loaded).
+__device__ __forceinline__ uint32_t seg_size_tc(const DevGraph& g, uint32_t v, uint32_t c, uint32_t lo, uint32_t hi,
+                                                uint32_t tc, int32_t t) {
+  if (tc == 0 || hi == lo) return hi - lo;
+  return seg_size_at(g, v, c, lo, hi, t);
 }
 
 // Driver segment of position np for prefix m (the smallest union-graph back
 // segment); false if some back segment is empty at batch time t.  `bytes`
 // receives 4 B x the sizes at time t of all back segments: the algorithmic
-// bytes of expanding this node.  Segment bounds are loaded four at a time.
+// bytes of expanding this node.  Segment bounds and touch counts are loaded
+// four back entries at a time.
 __device__ __forceinline__ bool pick_driver(const SearchParams& p, const PlanAnchor* A, uint32_t np,
                                             const uint32_t* m, int32_t t, uint32_t& dlo, uint32_t& dn,
                                             uint32_t& dsel, unsigned long long& bytes) {
@@ -163,27 +217,17 @@ __device__ __forceinline__ bool pick_driver(const SearchParams& p, const PlanAnc
   bool empty = false;
   unsigned long long b4 = 0;
   for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
-    uint32_t v[4], c[4];
-    uint64_t lo[4], hi[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const uint32_t b = b0 + (uint32_t)i;
-      lo[i] = 0; hi[i] = 0; v[i] = 0; c[i] = 0;
-      if (b < P.nb) {
-        v[i] = m[A->back_pos[P.boff + b]];
-        c[i] = A->back_combo[P.boff + b];
-        segment(p.g, v[i], c[i], lo[i], hi[i]);
-      }
-    }
+    SegQuad q;
+    load_quad(p.g, A, P, b0, m, 0xffffffffu, q);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const uint32_t b = b0 + (uint32_t)i;
       if (b >= P.nb) continue;
-      const uint32_t sz = (uint32_t)(hi[i] - lo[i]);
-      const uint32_t szt = seg_size_at(p.g, v[i], c[i], lo[i], hi[i], t);
+      const uint32_t sz = q.hi[i] - q.lo[i];
+      const uint32_t szt = seg_size_tc(p.g, q.v[i], q.c[i], q.lo[i], q.hi[i], q.tc[i], t);
       b4 += 4ull * szt;
       if (szt == 0) empty = true;
-      if (sz < best) { best = sz; dsel = b; dlo = (uint32_t)lo[i]; }
+      if (sz < best) { best = sz; dsel = b; dlo = q.lo[i]; }
     }
   }
   dn = best;
@@ -566,11 +610,16 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       act = false;
     }
     if (act) {
+      // the candidate and the first back segments of its position are loaded
+      // together: the segments depend on the prefix only
       x = pool[(uint64_t)L.dlo[e] + kk];
       m[0] = m0; m[1] = m1;
       uint32_t idx = e;
       for (int l2 = d; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
-      valid = check_candidate(p, pool, A, pos, x, m, L.dsel[e], (int32_t)t);
+      const uint32_t ds = L.dsel[e];
+      SegQuad q0;
+      load_quad(p.g, A, A->pos[pos], 0, m, ds, q0);
+      valid = check_candidate_q(p, pool, A, pos, x, m, ds, (int32_t)t, q0);
       if (valid && pos + 1 < n) {
         m[pos] = x;
         valid = pick_driver(p, A, pos + 1, m, (int32_t)t, ndlo, ndn, ndsel, nb4);
