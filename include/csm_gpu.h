@@ -67,7 +67,9 @@ extern "C" {
 
 /* ---- execution modes ------------------------------------------------ */
 #define CSM_MODE_BATCHED 0   /* many updates per launch sequence (default) */
-#define CSM_MODE_PLAIN 1     /* one update per launch sequence */
+#define CSM_MODE_PLAIN 1     /* one update per launch sequence: 2-3 launches for an update whose label
+                                triple matches no query edge, about 9 otherwise (index marks and one
+                                cooperative index round, seeds, search, results) */
 
 typedef struct csm_cfg {
   int32_t algorithm;          /* CSM_ALGO_* */
@@ -109,7 +111,9 @@ typedef struct csm_cfg {
 
 #define CSM_GRAPHS_OFF 0      /* launch every kernel of a batch from the host */
 #define CSM_GRAPHS_ON 1       /* capture a batch's launch sequence once per batch size and replay it
-                                 (search times are then not split out in csm_stats.search_ms) */
+                                 (search times are then not split out in csm_stats.search_ms); in
+                                 CSM_MODE_PLAIN only with attached queries or match-set output, the
+                                 other plain updates run their short sequences directly */
 
 /* Same 16-byte layout as the reference's InsertUnit fields
  * (ParaCOSM/CSM/utils/types.h:34-42). */

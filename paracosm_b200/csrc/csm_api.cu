@@ -77,6 +77,7 @@ struct csm_ctx {
   // graph
   bool has_graph = false;
   DevGraph g{};
+  std::vector<uint32_t> h_vlabel;  // folded vertex labels (kNone: no vertex), mirrored on the host
   uint64_t num_edges = 0;
   // candidate index
   IndexState index{};
@@ -373,14 +374,6 @@ __global__ void k_stamp(unsigned long long* stamp) {
   stamp[0] = t;
 }
 
-__global__ void k_latency(uint32_t B, const unsigned long long* stamp, csm_result* out) {
-  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= B) return;
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  out[s].latency_ns = t - stamp[0];
-}
-
 // ------------------------------------------------------------ batches
 //
 // One batch of B edge updates runs in phases.  The context that owns the
@@ -443,6 +436,8 @@ static void search_shape(const csm_ctx* q, uint32_t& warps, uint32_t& bps) {
   }
 }
 
+static int query_seed_search(csm_ctx* q, csm_ctx* o, uint32_t B, csm_result* out);
+
 // One standing query q over the owner o's union graph: index to the union
 // graph, seeds, search, per-update results; on q's stream.
 static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, csm_result* out) {
@@ -457,6 +452,16 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   if (q != o) CK(cudaMemsetAsync(c, 0, 64, st));
   int rc = index_apply_edges(q->index, g, o->d_ins2, L, st, &q->launches);
   if (rc) return rc;
+  return query_seed_search(q, o, B, out);
+}
+
+// Seeds, search and per-update results of query q over the owner o's graph
+// for the B updates described by o->d_info (the counters were cleared).
+static int query_seed_search(csm_ctx* q, csm_ctx* o, uint32_t B, csm_result* out) {
+  csm_ctx* ctx = q;  // launches are counted on the query's context
+  cudaStream_t st = q->st;
+  const DevGraph& g = o->g;
+  unsigned int* c = q->d_cnt;
   k_seed<<<blocks_for(B, 128), 128, 0, st>>>(B, o->d_info, g, q->d_plan, q->index.d2, q->index.words,
                                               q->d_tasks, c + 6, q->task_cap, q->d_safe, &g.ps->error,
                                               q->cfg.shard_rank, q->cfg.shard_count,
@@ -501,9 +506,9 @@ static int batch_query_search(csm_ctx* q, csm_ctx* o, uint32_t B, uint32_t L, cs
   }
   k_finalize<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_info, q->d_count, q->d_hash, q->d_bytes,
                                                   q->d_safe, q->d_stop, q->cfg.max_results, q->cfg.want_hash,
-                                                  out, (q->cfg.shard_count > 1 && q->cfg.shard_rank) ? 0u : 16u);
+                                                  out, (q->cfg.shard_count > 1 && q->cfg.shard_rank) ? 0u : 16u,
+                                                  o->d_stamp);
   CKL();
-  k_latency<<<blocks_for(B, 256), 256, 0, st>>>(B, o->d_stamp, out); CKL();
   return CSM_OK;
 }
 
@@ -557,6 +562,75 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   k_temporal_clear<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_rt, c + 5, g); CKL();
   ctx->batches++;
   for (csm_ctx* a : ctx->attached) a->batches++;
+  return CSM_OK;
+}
+
+// ------------------------------------------------- one update per launch
+//
+// The plain form (CSM_MODE_PLAIN) runs each edge update as its own short
+// launch sequence.  An edge whose label triple (L(v1), L(v2), label) matches
+// no query edge can neither be part of an embedding nor change a candidate
+// index (every index condition counts only edges whose label triple matches
+// a query edge), so such an update mutates the graph and reports zero; the
+// host decides this from its mirror of the vertex labels.  A deletion counts
+// with the edge's own label, which the host does not know, so a deletion is
+// only decided this way when no query edge has its vertex-label pair.
+// Launches per update:
+//   no matching query edge: resolve, [compaction copy,] mutate        2-3
+//   insertion:  resolve, compaction copy, mutate, index marks + round,
+//               seeds, search queue + search, results                 9
+//   deletion:   resolve, seeds, search queue + search, results,
+//               mutate, index marks + round                           8
+// (the compaction copy returns at once unless the insertion's relocation
+// does not fit; GraphFlow has no index rounds).
+
+// True when some query edge may match the update's label triple.
+static bool plain_may_count(const csm_ctx* ctx, const csm_update& u) {
+  const DevGraph& g = ctx->g;
+  if (u.type != 'e' || u.id1 >= g.n || u.id2 >= g.n || u.id1 == u.id2) return false;  // INVALID
+  const uint32_t L1 = ctx->h_vlabel[u.id1], L2 = ctx->h_vlabel[u.id2];
+  if (L1 == kNone || L2 == kNone) return false;
+  const uint32_t el = fold_host(ctx->qlab_e, u.label);
+  const Plan* P = ctx->h_plan;
+  for (uint32_t a = 0; a < P->n_anchor; a++) {
+    const PlanAnchor& A = P->anchors[a];
+    if (u.is_add && A.el != el) continue;
+    if ((A.la == L1 && A.lb == L2) || (A.la == L2 && A.lb == L1)) return true;
+  }
+  return false;
+}
+
+// One edge update of the plain form (no attached queries); d_up is the record
+// in device memory, h its host copy.
+static int run_plain_edge(csm_ctx* ctx, const csm_update* d_up, const csm_update& h, csm_result* out) {
+  cudaStream_t st = ctx->st;
+  const DevGraph& g = ctx->g;
+  uint64_t* keys = ctx->d_ins2;
+  k_plain_resolve<<<1, 32, 0, st>>>(d_up, g, ctx->d_info, keys, ctx->d_cnt, ctx->d_count, ctx->d_hash, ctx->d_bytes,
+                                     ctx->d_stop);
+  CKL();
+  if (h.type == 'e' && h.is_add) {
+    k_compact_copy<<<ctx->sm_count * 4, 1024, 0, st>>>(g);  // returns at once unless the pool must be compacted
+    CKL();
+  }
+  int rc = CSM_OK;
+  if (!plain_may_count(ctx, h)) {
+    k_plain_mutate<<<1, 256, 0, st>>>(g, ctx->d_info, keys, out, ctx->d_stamp, 16u);
+    CKL();
+  } else if (h.is_add) {
+    k_plain_mutate<<<1, 256, 0, st>>>(g, ctx->d_info, keys, nullptr, nullptr, 16u);
+    CKL();
+    rc = index_apply_edge_one(ctx->index, g, keys, st, &ctx->launches);
+    if (!rc) rc = query_seed_search(ctx, ctx, 1, out);
+  } else {
+    rc = query_seed_search(ctx, ctx, 1, out);
+    if (rc) return rc;
+    k_plain_mutate<<<1, 256, 0, st>>>(g, ctx->d_info, keys, nullptr, nullptr, 16u);
+    CKL();
+    rc = index_apply_edge_one(ctx->index, g, keys, st, &ctx->launches);
+  }
+  if (rc) return rc;
+  ctx->batches++;
   return CSM_OK;
 }
 
@@ -760,10 +834,24 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
   while (i < n) {
     for (size_t k = 0; k < ctx->attached.size(); k++) out_q[k] = ctx->attached[k]->d_results + i;
     if (h[i].type == 'v') {
+      // the host's mirror of the vertex labels follows the device
+      // (k_vertex_update and run_vertex_delete)
+      const uint32_t vid = h[i].id1;
+      const bool was_added = h[i].is_add && vid < ctx->g.n_cap && ctx->h_vlabel[vid] == kNone;
+      const bool removed = !h[i].is_add && vid < ctx->g.n;
       rc = run_vertex_update(ctx, d_ups + i, h[i], ctx->d_results + i, out_q);
       if (rc) return rc;
+      if (was_added) ctx->h_vlabel[vid] = fold_host(ctx->qlab_v, h[i].label);
+      if (removed) ctx->h_vlabel[vid] = kNone;
       ctx->v_updates++;
       for (csm_ctx* a : ctx->attached) a->v_updates++;
+      i++;
+      continue;
+    }
+    if (ctx->cfg.mode == CSM_MODE_PLAIN && ctx->attached.empty() && !ctx->d_enum) {
+      rc = run_plain_edge(ctx, d_ups + i, h[i], ctx->d_results + i);
+      if (rc) return rc;
+      ctx->e_updates++;
       i++;
       continue;
     }
@@ -1365,6 +1453,9 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
   g.n_qe = (uint32_t)ctx->qlab_e.size();
   CK(cudaMemsetAsync(g.vlabel, 0xff, 4ull * n_cap, st));
   CK(cudaMemcpyAsync(g.vlabel, vlabels, 4ull * n_v, cudaMemcpyHostToDevice, st));
+  ctx->h_vlabel.assign(n_cap, kNone);
+  for (uint32_t v = 0; v < n_v; v++)
+    if (vlabels[v] != kNone) ctx->h_vlabel[v] = fold_host(ctx->qlab_v, vlabels[v]);
   if (n_v) { k_fold_vlabels<<<blocks_for(n_v, 256), 256, 0, st>>>(g.vlabel, n_v, g); CKL(); }
   CK(cudaMemsetAsync(g.row_off, 0, 8ull * n_cap, st));
   CK(cudaMemsetAsync(g.row_cap, 0, 4ull * n_cap, st));

@@ -13,10 +13,14 @@
 //               definition: one warp per 64-vertex word; short segments are
 //               scanned by one lane each, long ones by the whole warp with
 //               an early exit on the first supporting neighbour
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstring>
 
 #include "csm_index.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace csm {
 
@@ -125,11 +129,8 @@ __global__ void k_ix_seed_vertex(uint32_t v, const IxDag* __restrict__ dag, IxBi
 // Phase 1 (d1 of u): for each parent p, every vertex w whose d1[p] changed
 // marks its neighbours in S(w, L(u), l(u,p)).  Phase 2 (d2 of u): the same
 // from each child c through d2[c] changes.  One warp per word of changes.
-__global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase) {
-  if (!*b.active) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+__device__ __forceinline__ void ix_prop(const DevGraph& g, const IxDag* __restrict__ dag, const IxBits& b, uint32_t u,
+                                        uint32_t phase, uint32_t lane, uint32_t warp, uint32_t nwarps) {
   const uint32_t* pool = g.pools[g.ps->active];
   const uint32_t nsrc = phase == 1 ? dag->npar[u] : dag->nchd[u];
   uint64_t* dst = (phase == 1 ? b.m1 : b.m2) + (uint64_t)u * b.words;
@@ -153,15 +154,18 @@ __global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
   }
 }
 
+__global__ void k_ix_prop(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase) {
+  if (!*b.active) return;
+  ix_prop(g, dag, b, u, phase, threadIdx.x & 31, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+          (gridDim.x * blockDim.x) >> 5);
+}
+
 // Re-evaluates the marked flags of query vertex u (phase 1: d1, phase 2: d2).
 // full = 1 evaluates every vertex of u's label (index build).  Each warp owns
 // whole words of the target bitset, so its updates need no atomics.
-__global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase,
-                          uint32_t full) {
-  if (!*b.active) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+__device__ __forceinline__ void ix_eval(const DevGraph& g, const IxDag* __restrict__ dag, const IxBits& b, uint32_t u,
+                                        uint32_t phase, uint32_t full, uint32_t lane, uint32_t warp,
+                                        uint32_t nwarps) {
   const uint32_t* pool = g.pools[g.ps->active];
   const uint32_t lu = dag->qlab[u];
   const uint64_t off = (uint64_t)u * b.words;
@@ -249,9 +253,56 @@ __global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, u
   }
 }
 
+__global__ void k_ix_eval(DevGraph g, const IxDag* __restrict__ dag, IxBits b, uint32_t u, uint32_t phase,
+                          uint32_t full) {
+  if (!*b.active) return;
+  ix_eval(g, dag, b, u, phase, full, threadIdx.x & 31, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+          (gridDim.x * blockDim.x) >> 5);
+}
+
 // End of a round: the change bitsets start the next round empty.
 __global__ void k_ix_clear_changes(IxBits b, uint64_t n) {
   if (!*b.active) return;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    b.c1[i] = 0;
+    b.c2[i] = 0;
+  }
+}
+
+// One incremental round over every query vertex in a single launch, for the
+// changes of one edge update (the plain form): the steps of
+// index_launch_round -- per query vertex in DAG order, propagation of the
+// parents' d1 changes and re-evaluation of d1, then in reverse order the
+// children's d2 changes and d2 -- separated by grid-wide barriers instead of
+// kernel boundaries.  Launched cooperatively (every block resident), with a
+// grid no larger than the occupancy allows.  Every block takes the same
+// branches, so every block reaches every barrier.
+__global__ void __launch_bounds__(256) k_ix_round_coop(DevGraph g, const IxDag* __restrict__ dag, IxBits b,
+                                                       IxOrder ord) {
+  if (!*b.active) return;  // nothing that the flags depend on changed: the same in every block
+  cg::grid_group grid = cg::this_grid();
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = 0; i < ord.nq; i++) {
+    const uint32_t u = ord.order[i];
+    if (dag->npar[u] != 0) {  // the root's d1 is its label test: only new vertices change it
+      ix_prop(g, dag, b, u, 1, lane, warp, nwarps);
+      grid.sync();
+    }
+    ix_eval(g, dag, b, u, 1, 0, lane, warp, nwarps);
+    grid.sync();
+  }
+  for (uint32_t i = ord.nq; i-- > 0;) {
+    const uint32_t u = ord.order[i];
+    if (dag->nchd[u] != 0) {
+      ix_prop(g, dag, b, u, 2, lane, warp, nwarps);
+      grid.sync();
+    }
+    ix_eval(g, dag, b, u, 2, 0, lane, warp, nwarps);
+    grid.sync();
+  }
+  const uint64_t n = (uint64_t)ord.nq * b.words;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     b.c1[i] = 0;
     b.c2[i] = 0;
@@ -554,6 +605,31 @@ int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, u
   k_ix_seed<<<(L + 255) / 256, 256, 0, st>>>(keys, L, g, ix.d_dag, ix.bits);
   (*launches)++;
   return index_launch_round(ix, g, st, launches, false);
+}
+
+int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys, cudaStream_t st,
+                         uint64_t* launches) {
+  if (!ix.active) return CSM_OK;
+  if (!ix.coop_blocks) {
+    int occ = 0;
+    IXCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ix_round_coop, 256, 0));
+    const uint64_t warps_needed = std::max<uint64_t>(ix.words, 1);
+    ix.coop_blocks = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((warps_needed + 7) / 8, (uint64_t)ix.sm_count * (uint64_t)std::max(occ, 1)));
+  }
+  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
+  k_ix_seed<<<1, 32, 0, st>>>(keys, 2, g, ix.d_dag, ix.bits);
+  (*launches)++;
+  IxOrder ord{};
+  ord.nq = ix.h_dag.nq;
+  for (uint32_t i = 0; i < ord.nq; i++) ord.order[i] = ix.order[i];
+  DevGraph gv = g;
+  const IxDag* dag = ix.d_dag;
+  IxBits bits = ix.bits;
+  void* args[] = {&gv, &dag, &bits, &ord};
+  IXCK(cudaLaunchCooperativeKernel((const void*)k_ix_round_coop, dim3(ix.coop_blocks), dim3(256), args, 0, st));
+  (*launches)++;
+  return CSM_OK;
 }
 
 int index_vertex_update(IndexState& ix, const DevGraph& g, const csm_update& h, cudaStream_t st, uint64_t* launches) {

@@ -79,8 +79,15 @@ struct IxBits {
   unsigned int* active;  // nonzero when the current round marked anything; else its kernels return at once
 };
 
+// Query vertices in DAG order, by value for a kernel argument.
+struct IxOrder {
+  uint32_t nq;
+  uint32_t order[kMaxQ];
+};
+
 struct IndexState {
   int algo = CSM_ALGO_GRAPHFLOW;
+  uint32_t coop_blocks = 0;  // grid of the single-launch round (0: not sized yet)
   bool active = false;
   uint64_t* d2 = nullptr;     // == bits.d2 (null: no index)
   uint64_t words = 0;
@@ -100,6 +107,11 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
 // keys[0, L) (packed (x, combo, y), sentinel-padded) changed.
 int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,
                       uint64_t* launches);
+// The same for the two directed entries keys[0..1] of one edge update, in two
+// launches: the marks, then every propagation and re-evaluation step in one
+// cooperative kernel.
+int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys, cudaStream_t st,
+                         uint64_t* launches);
 int index_vertex_update(IndexState& ix, const DevGraph& g, const csm_update& h, cudaStream_t st, uint64_t* launches);
 int index_counts(IndexState& ix, cudaStream_t st, uint64_t* d1_count, uint64_t* d2_count);
 void index_stats(const IndexState& ix, uint64_t* entries, uint64_t* vertices);

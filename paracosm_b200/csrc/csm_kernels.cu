@@ -494,6 +494,146 @@ void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const
   k_mut_delete_g<256><<<big_blocks, 256, 0, st>>>(ranges, n_ranges, del_key, del_pos, g);
 }
 
+// ------------------------------------------------- one update per launch
+//
+// The plain form runs each edge update on its own.  A batch of one needs no
+// sorting, no grouping by edge and no temporal entries: an insertion is
+// searched after its edge is added and a deletion before its edge is
+// removed, so the graph at search time is the sequential one.  Its
+// preparation is one kernel and its row mutation another (plus the
+// compaction copy when an insertion's relocation does not fit).
+
+__global__ void k_plain_resolve(const csm_update* up, DevGraph g, UpdInfo* info, uint64_t* keys, unsigned int* cnt,
+                                unsigned long long* count, unsigned long long* hash, unsigned long long* bytes,
+                                unsigned int* stop) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const csm_update u = *up;
+  UpdInfo inf;
+  inf.v1 = u.id1; inf.v2 = u.id2; inf.label = fold_elabel(g, u.label); inf.flags = 0;
+  keys[0] = ~0ULL; keys[1] = ~0ULL;
+  for (int i = 0; i < 16; i++) cnt[i] = 0;
+  count[0] = 0; hash[0] = 0; bytes[0] = 0; stop[0] = 0;
+  PoolState* ps = g.ps;
+  ps->need = 0;
+  ps->compact = 0;
+  if (u.type == 'e') {
+    const bool ok = u.id1 < g.n && u.id2 < g.n && u.id1 != u.id2 && g.vlabel[u.id1] != kNone &&
+                    g.vlabel[u.id2] != kNone;
+    if (!ok) {
+      inf.flags = UF_INVALID;
+    } else {
+      inf.flags = UF_VALID | (u.is_add ? UF_ADD : 0u);
+      const uint32_t l0 = find_label(g, g.pools[ps->active], u.id1, u.id2);
+      const uint32_t x = min(u.id1, u.id2), y = max(u.id1, u.id2);
+      if (u.is_add) {
+        if (l0 != kNone) {
+          inf.flags |= UF_DUP;  // graph unchanged; counted with the given label
+        } else {
+          inf.flags |= UF_MUT;
+          keys[0] = g.kb.pack(x, g.vlabel[y] * g.n_el + inf.label, y);
+          keys[1] = g.kb.pack(y, g.vlabel[x] * g.n_el + inf.label, x);
+          unsigned long long need = 0;
+          const uint32_t ends[2] = {x, y};
+          for (int k = 0; k < 2; k++) {
+            const uint32_t v = ends[k];
+            const uint32_t deg = g.dir[(size_t)v * (g.nc + 1) + g.nc];
+            if (deg + 1 > g.row_cap[v]) need += grow_cap(deg + 1);
+          }
+          ps->need = need;
+          ps->compact = (need > g.pool_cap - ps->top[ps->active]) ? 1u : 0u;
+        }
+      } else if (l0 == kNone) {
+        inf.flags |= UF_INVALID;  // deleting a missing edge
+      } else {
+        inf.label = l0;  // a deletion counts with the edge's own label
+        inf.flags |= UF_MUT;
+        keys[0] = g.kb.pack(x, g.vlabel[y] * g.n_el + l0, y);
+        keys[1] = g.kb.pack(y, g.vlabel[x] * g.n_el + l0, x);
+      }
+    }
+  }
+  info[0] = inf;
+}
+
+__global__ void __launch_bounds__(256) k_plain_mutate(DevGraph g, const UpdInfo* info, const uint64_t* keys,
+                                                      csm_result* out, const unsigned long long* stamp,
+                                                      uint32_t mut_bytes) {
+  PoolState* ps = g.ps;
+  const uint32_t lane = threadIdx.x;
+  __shared__ unsigned long long s_off;
+  __shared__ uint32_t s_pos, s_bad;
+  if (lane == 0) {
+    if (ps->compact) {  // k_compact_copy moved every row to the other pool (k_compact_finish's step)
+      ps->top[ps->active] = 0;
+      ps->active = 1u - ps->active;
+      ps->compact = 0;
+    }
+    ps->need = 0;
+  }
+  __syncthreads();
+  const UpdInfo inf = info[0];
+  uint32_t* pool = g.pools[ps->active];
+  if (inf.flags & UF_MUT) {
+    const bool add = (inf.flags & UF_ADD) != 0;
+    for (int k = 0; k < 2; k++) {
+      const uint64_t key = keys[k];
+      const uint32_t x = g.kb.x_of(key), c = g.kb.c_of(key), y = g.kb.y_of(key);
+      uint32_t* dirx = g.dir + (size_t)x * (g.nc + 1);
+      const uint32_t deg = dirx[g.nc];
+      const uint64_t off = g.row_off[x];
+      if (lane == 0) {
+        s_pos = (uint32_t)lower_bound_u32(pool + off, dirx[c], dirx[c + 1], y);
+        s_bad = 0;
+        if (!add && (s_pos >= dirx[c + 1] || pool[off + s_pos] != y)) s_bad = 1;  // the entry must be there
+      }
+      __syncthreads();
+      const uint32_t p = s_pos;
+      if (s_bad) {
+        if (lane == 0) atomicExch(&ps->error, kErrRowState);
+        break;
+      }
+      if (add) {
+        uint64_t dst = off;
+        uint32_t new_cap = 0;
+        if (deg + 1 > g.row_cap[x]) {
+          new_cap = grow_cap(deg + 1);
+          if (lane == 0) {
+            unsigned long long o = atomicAdd(&ps->top[ps->active], (unsigned long long)new_cap);
+            if (o + new_cap > g.pool_cap) { atomicExch(&ps->error, kErrPoolFull); o = ~0ULL; }
+            s_off = o;
+          }
+          __syncthreads();
+          dst = s_off;
+          if (dst == ~0ULL) break;  // the same value in every thread
+          group_move_left<256>(pool, off, dst, p, lane);                 // different rows: no overlap
+          group_move_left<256>(pool, off + p, dst + p + 1, deg - p, lane);
+        } else {
+          group_move_right<256>(pool, off + p, off + p + 1, deg - p, lane);
+        }
+        if (lane == 0) pool[dst + p] = y;
+        for (uint32_t cc = c + 1 + lane; cc <= g.nc; cc += 256) dirx[cc] += 1;
+        if (lane == 0 && new_cap) { g.row_off[x] = dst; g.row_cap[x] = new_cap; }
+      } else {
+        group_move_left<256>(pool, off + p + 1, off + p, deg - p - 1, lane);
+        for (uint32_t cc = c + 1 + lane; cc <= g.nc; cc += 256) dirx[cc] -= 1;
+      }
+      __syncthreads();
+    }
+  }
+  if (out && lane == 0) {
+    // an update whose label triple matches no query edge: nothing to count
+    csm_result r;
+    r.pos = 0; r.neg = 0; r.hash = 0;
+    r.status = (inf.flags & UF_INVALID) ? CSM_ST_INVALID : CSM_ST_OK;
+    r.safe = 1;
+    r.work_bytes = (inf.flags & UF_MUT) ? (unsigned long long)mut_bytes : 0ull;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    r.latency_ns = stamp ? t - stamp[0] : 0ull;
+    out[0] = r;
+  }
+}
+
 // Vertex deletion: the packed keys of every directed entry incident to v,
 // (v, combo, y) and (y, combo', v), for the deletion kernels.
 __global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys) {

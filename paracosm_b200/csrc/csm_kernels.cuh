@@ -50,6 +50,18 @@ void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const
                        uint32_t* del_pos, const DevGraph& g, uint32_t warp_blocks, uint32_t big_blocks,
                        cudaStream_t st);
 __global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys);
+
+// ---- one edge update per launch sequence (the plain form; csm_kernels.cu) ----
+// keys[0..1]: the update's two directed entries (sentinels when the graph does
+// not change); cnt[0..15], count/hash/bytes/stop[0]: cleared for the search.
+__global__ void k_plain_resolve(const csm_update* up, DevGraph g, UpdInfo* info, uint64_t* keys, unsigned int* cnt,
+                                unsigned long long* count, unsigned long long* hash, unsigned long long* bytes,
+                                unsigned int* stop);
+// Applies the update's row insertion or deletion (one 256-thread block), after
+// finishing a compaction k_compact_copy ran; with `out`, also writes the
+// result of an update that needs no search (latency from stamp[0]).
+__global__ void k_plain_mutate(DevGraph g, const UpdInfo* info, const uint64_t* keys, csm_result* out,
+                               const unsigned long long* stamp, uint32_t mut_bytes);
 __global__ void k_vertex_update(const csm_update* ups, uint32_t B, DevGraph g, UpdInfo* info);
 
 // ---- search (csm_search.cu) ----
@@ -153,7 +165,8 @@ void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
                            const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out,
-                           uint32_t mut_bytes = 16);  // bytes of an applied mutation (0 on secondary shards)
+                           uint32_t mut_bytes = 16,  // bytes of an applied mutation (0 on secondary shards)
+                           const unsigned long long* stamp = nullptr);  // non-null: latency from stamp[0]
 // stop[] values: 1 = the cap was reached, 2 = the deadline passed first
 constexpr unsigned int kStopCap = 1u, kStopDeadline = 2u;
 __global__ void k_classify(uint64_t n, const csm_update* ups, DevGraph g, const Plan* plan, uint8_t* safe);

@@ -1011,7 +1011,7 @@ void launch_search(const SearchParams& p, uint32_t n_q, uint32_t blocks, uint32_
 __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long long* count,
                            const unsigned long long* hash, const unsigned long long* bytes, const uint32_t* safe,
                            const unsigned int* stop, uint64_t cap, int want_hash, csm_result* out,
-                           uint32_t mut_bytes) {
+                           uint32_t mut_bytes, const unsigned long long* stamp) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= B) return;
   const UpdInfo u = info[s];
@@ -1029,6 +1029,7 @@ __global__ void k_finalize(uint32_t B, const UpdInfo* info, const unsigned long 
     if (want_hash && r.status == CSM_ST_OK) r.hash = hash[s];
     r.work_bytes = (bytes ? bytes[s] : 0ull) + ((u.flags & UF_MUT) ? (unsigned long long)mut_bytes : 0ull);
   }
+  if (stamp) r.latency_ns = global_ns() - stamp[0];
   out[s] = r;
 }
 

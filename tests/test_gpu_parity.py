@@ -282,3 +282,33 @@ def test_poll_reports_completion_without_blocking():
         res = eng.results(first, len(g["stream"]))
     x = g["exp"]
     assert_same(res, x["symbi_pos"], x["symbi_neg"], x["symbi_hash"])
+
+
+@pytest.mark.parametrize("algo", ["parallel_graphflow", "parallel_symbi", "parallel_turboflux", "parallel_calig"])
+def test_plain_form_launches_per_update(algo):
+    """One update per launch sequence: an update whose label triple matches no query edge costs at
+    most 3 kernel launches (resolve, compaction copy for an insertion, row mutation), any other at
+    most 10 (its index round is one cooperative launch); counts stay those of the reference."""
+    g = load_golden("mixed_2el")
+    qv, qe = g["qv"], g["qe"]
+    trip, pair = set(), set()
+    for a, b, l in qe:
+        trip |= {(qv[a], qv[b], l), (qv[b], qv[a], l)}
+        pair |= {(qv[a], qv[b]), (qv[b], qv[a])}
+    x = g["exp"]
+    with Engine(algo, mode="plain") as eng:
+        eng.set_query(qv, qe)
+        eng.load_graph(g["vl"], g["e"])
+        eng.build_index()
+        seen = {True: 0, False: 0}
+        for i, u in enumerate(g["stream"]):
+            l0 = eng.kernel_launches()
+            r = eng.run(g["stream"][i:i + 1])[0]
+            launches = eng.kernel_launches() - l0
+            l1, l2 = g["vl"][u["id1"]], g["vl"][u["id2"]]
+            may = (l1, l2, u["label"]) in trip if u["is_add"] else (l1, l2) in pair
+            assert launches <= (10 if may else 3), (i, launches, may)
+            seen[may] += 1
+            if algo != "parallel_calig":
+                assert (int(r["pos"]), int(r["neg"])) == (int(x["symbi_pos"][i]), int(x["symbi_neg"][i])), i
+        assert seen[True] > 20 and seen[False] > 20
