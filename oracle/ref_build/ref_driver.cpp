@@ -1,5 +1,11 @@
 // Sequential-semantics driver for the reference ParaCOSM plugins.
 //
+// Built a second time with -DCSM_GPU_PLUGIN (oracle/_ref/ref_driver_gpu), it
+// also accepts -a gpu_graphflow / gpu_turboflux / gpu_symbi / gpu_calig /
+// gpu_newsp: the CUDA engine as a `matching` subclass (include/
+// csm_gpu_plugin.h), driven by this same loop through the reference's
+// plugin interface.
+//
 // Test infrastructure only: this program links the UNMODIFIED reference plugin
 // objects (compiled from the reference sources by oracle/ref_build/Makefile)
 // and drives them the way the reference's dead `SingleThreadUpdate` loop does
@@ -48,6 +54,10 @@
 #include "matching/matching.h"
 #include "utils/globals.h"
 #include "utils/types.h"
+#ifdef CSM_GPU_PLUGIN
+// the engine behind the reference's plugin interface (include/csm_gpu_plugin.h)
+#include "csm_gpu_plugin.h"
+#endif
 
 // ref_index_access.cpp: the sequential SymBi / TurboFlux index state
 bool ref_dump_index(matching* m, const std::string& algo, uint32_t nq, FILE* f, long at);
@@ -222,6 +232,13 @@ int main(int argc, char** argv) {
   else if (a.algo == "parallel_symbi") mm = new Parrllel_SymBi(query, data, maxr, false, print_enum, a.homo, orders, a.threads, a.auto_tuning);
   else if (a.algo == "parallel_turboflux") mm = new Parallel_TurboFlux(query, data, maxr, false, print_enum, a.homo, a.threads, a.auto_tuning);
   else if (a.algo == "parallel_graphflow") mm = new Parallel_Graphflow(query, data, maxr, false, print_enum, a.homo, a.threads, a.auto_tuning);
+#ifdef CSM_GPU_PLUGIN
+  else if (a.algo == "gpu_graphflow") mm = new GpuPlugin(query, data, maxr, false, print_enum, a.homo, CSM_ALGO_GRAPHFLOW);
+  else if (a.algo == "gpu_turboflux") mm = new GpuPlugin(query, data, maxr, false, print_enum, a.homo, CSM_ALGO_TURBOFLUX);
+  else if (a.algo == "gpu_symbi") mm = new GpuPlugin(query, data, maxr, false, print_enum, a.homo, CSM_ALGO_SYMBI);
+  else if (a.algo == "gpu_calig") mm = new GpuPlugin(query, data, maxr, false, print_enum, a.homo, CSM_ALGO_CALIG);
+  else if (a.algo == "gpu_newsp") mm = new GpuPlugin(query, data, maxr, false, print_enum, a.homo, CSM_ALGO_NEWSP);
+#endif
   else { fprintf(stderr, "Unknown algorithm %s\n", a.algo.c_str()); return 2; }
 
   EnumHashBuf hb(query.NumVertices());
