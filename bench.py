@@ -65,9 +65,9 @@ CONFIGS = {
         "preset": "c5", "algo": "parallel_symbi", "batch": 8192, "max_results": 1_000_000,
         "min_updates": 500_000, "deadline_ns": 1_000_000_000,
         "workload": "RMAT 2^24 V, avg deg 32 (268M edges), 32 vlabels Zipf(1.0), 4 elabels; 24- and 32-vertex "
-                    "queries (sparse and dense) as four standing queries on one graph, plugins CaLiG-style / "
-                    "TurboFlux / SymBi / CaLiG-style; 90/10 insert/delete stream; per update max_results 1e6 and a "
-                    "1 s limit",
+                    "queries (sparse and dense) as four standing queries on one graph, the CaLiG-style plugin on the "
+                    "24-vertex sparse and 32-vertex dense ones, the NewSP-style plugin on the other two; 90/10 "
+                    "insert/delete stream; per update max_results 1e6 and a 1 s limit",
     },
     "c1": {
         "preset": "c1", "algo": "parallel_graphflow", "batch": 2000, "max_results": 0, "min_updates": 2000,
@@ -361,73 +361,87 @@ def run_reference_arm(args, cfg):
 
 def serve_sweep(w, cfg, rates, seconds, *, n_queries, device=0, plugins=None, cap=None,
                 deadline_ms=None) -> list[dict]:
-    """Runs the serving loop (paracosm_b200/_bin/csm_serve) on the workload at each offered rate."""
+    """Runs the serving loop (paracosm_b200/_bin/csm_serve) on the workload: one process, one set-up,
+    then `seconds` of Poisson arrivals at each offered rate in turn (each segment continues the
+    stream where the last one stopped).  One dict per rate."""
     exe = ROOT / "paracosm_b200" / "_bin" / "csm_serve"
-    out = []
-    for r in rates:
-        cmd = [str(exe), "-w", str(w.directory), "--queries", str(n_queries), "--rate", str(r),
-               "--max-seconds", str(seconds), "--max-batch", str(cfg["batch"]), "--device", str(device),
-               "--cap", str(cfg["max_results"] if cap is None else cap),
-               "--plugins", ",".join(plugins or [cfg["algo"]]), "--graphs", "1"]
-        if deadline_ms:
-            cmd += ["--deadline-ms", str(deadline_ms)]
-        t0 = time.perf_counter()
-        try:
-            p = subprocess.run(cmd, capture_output=True, text=True, timeout=max(180.0, 30 * seconds))
-        except subprocess.TimeoutExpired:
-            out.append({"offered_rate": r, "error": f"serving run exceeded {max(180.0, 30 * seconds):.0f}s"})
-            continue
-        if p.returncode != 0:
-            out.append({"offered_rate": r, "error": p.stderr[-300:]})
-            continue
-        d = json.loads(p.stdout.strip().splitlines()[-1])
-        d["wall_s"] = time.perf_counter() - t0
-        out.append(d)
-        log(f"serve rate {r:g}: sustained {d['sustained']:.0f} upd/s p50 {d['p50_us']:.0f} us "
+    cmd = [str(exe), "-w", str(w.directory), "--queries", str(n_queries), "--rates", ",".join(f"{r:g}" for r in rates),
+           "--max-seconds", str(seconds), "--max-batch", str(cfg["batch"]), "--device", str(device),
+           "--cap", str(cfg["max_results"] if cap is None else cap),
+           "--plugins", ",".join(plugins or [cfg["algo"]]), "--graphs", "1"]
+    if deadline_ms:
+        cmd += ["--deadline-ms", str(deadline_ms)]
+    t0 = time.perf_counter()
+    limit = 600.0 + 60.0 * seconds * len(rates)
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=limit)
+    except subprocess.TimeoutExpired:
+        return [{"offered_rate": r, "error": f"serving run exceeded {limit:.0f}s"} for r in rates]
+    if p.returncode != 0:
+        return [{"offered_rate": r, "error": p.stderr[-300:]} for r in rates]
+    out = [json.loads(line) for line in p.stdout.strip().splitlines() if line.startswith('{"segment"')]
+    wall = time.perf_counter() - t0
+    for d in out:
+        d["process_wall_s"] = wall
+        log(f"serve rate {d['offered_rate']:g}: sustained {d['sustained']:.0f} upd/s p50 {d['p50_us']:.0f} us "
             f"p99 {d['p99_us']:.0f} us mean batch {d['mean_batch']:.0f}")
     return out
 
 
+C4_PLUGINS = ["parallel_symbi", "parallel_turboflux", "parallel_graphflow"]
+C5_PLUGINS = ["parallel_calig", "parallel_newsp", "parallel_newsp", "parallel_calig"]
+
+
+def c4_leg(rates, seconds, device=0) -> dict:
+    """C4: 64 standing queries (sizes 4-32, half sparse, half dense, round-robin over the three
+    plugins) on the 2^22-vertex graph, Poisson arrivals swept over the offered rates, admission
+    against a 40 GB budget, with the per-update cap and search limit named in the config."""
+    cfg = CONFIGS["c4"]
+    w = get_workload(cfg, cfg["min_updates"])
+    sweep = serve_sweep(w, cfg, rates, seconds, n_queries=64, plugins=C4_PLUGINS,
+                        deadline_ms=cfg.get("deadline_ms"), device=device)
+    ok = [d for d in sweep if "sustained" in d]
+    best = max(ok, key=lambda d: d["sustained"]) if ok else None
+    return {"workload": cfg["workload"], "queries": 64, "plugins": C4_PLUGINS, "max_results": cfg["max_results"],
+            "deadline_ms": cfg["deadline_ms"], "budget_gb": 40, "seconds_per_rate": seconds,
+            "sustained_best": best["sustained"] if best else None,
+            "p50_us_at_best": best["p50_us"] if best else None, "p99_us_at_best": best["p99_us"] if best else None,
+            "sweep": sweep,
+            "note": "max_results 1e4 and a 100 ms search limit per update are not in the config's text: with the "
+                    "1e6 cap of the 2^22-vertex SymBi config, 32-vertex sparse queries reach the cap on most "
+                    "updates and a first batch does not finish"}
+
+
 def run_serving_config(args, cfg):
-    """C4: 64 standing queries (sizes 4-32, half sparse, half dense, round-robin over the
-    three plugins) on the C3 graph, Poisson arrivals swept over offered loads, admission
-    against a 40 GB budget.  value = the highest sustained updates/s of the sweep."""
+    """C4 on its own: value = the highest sustained updates/s of the sweep."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = get_workload(cfg, cfg["min_updates"])
-    plugins = ["parallel_symbi", "parallel_turboflux", "parallel_graphflow"]
     rates = [float(r) for r in (args.serve_rates or "1e4,1e5,1e6").split(",") if r]
-    sweep = serve_sweep(w, cfg, rates, args.serve_seconds, n_queries=64, plugins=plugins,
-                        deadline_ms=cfg.get("deadline_ms"))
-    ok = [d for d in sweep if "sustained" in d]
-    best = max(ok, key=lambda d: d["sustained"]) if ok else None
-    line = {"metric": METRIC, "value": best["sustained"] if best else None, "unit": "updates/s", "n_gpus": 1,
+    leg = c4_leg(rates, args.serve_seconds)
+    line = {"metric": METRIC, "value": leg["sustained_best"], "unit": "updates/s", "n_gpus": 1,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": cfg["workload"], "batch": cfg["batch"], "max_results": cfg["max_results"]},
-            "p50_us": best["p50_us"] if best else None, "p99_us": best["p99_us"] if best else None,
-            "serving": sweep}
+            "p50_us": leg["p50_us_at_best"], "p99_us": leg["p99_us_at_best"], "serving": leg["sweep"], "c4": leg}
     print(json.dumps(line), flush=True)
 
 
-def run_stress_config(args, cfg):
-    """C5: four large standing queries on one 2^24-vertex graph, batches of 8,192 updates, a
-    per-update cap of 1e6 and a 1 s limit.  value = updates/s over the timed batches;
-    success rate = share of (update, query) results that are neither CAPPED nor TIMED_OUT."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    import torch  # noqa: F401  (CUDA context order as in the main path)
+def c5_leg(warmup: int, steps: int, device=0) -> dict:
+    """C5: the four large queries (24 and 32 vertices, sparse and dense) as standing queries on one
+    2^24-vertex graph, run by the CaLiG-style and NewSP-style plugins (each takes one sparse and one
+    dense query), batches of 8,192 updates, per update a cap of 1e6 matches and a 1 s limit.
+    updates/s from CUDA events on the owner's stream (the attached queries' streams join it);
+    success rate = share of (update, query) results neither CAPPED nor TIMED_OUT."""
+    import torch
 
     from paracosm_b200 import ST_CAPPED, ST_TIMED_OUT, Engine
-    B, W, K = cfg["batch"], args.warmup, args.steps
+    cfg = CONFIGS["c5"]
+    B, W, K = cfg["batch"], warmup, steps
     w = get_workload(cfg, max(cfg["min_updates"], (W + K) * B))
-    # the CaLiG-style plugin on two of the four queries (C5 names the CaLiG- and
-    # NewSP-style plugins; there is no NewSP-style plugin here)
-    plugins = ["parallel_calig", "parallel_turboflux", "parallel_symbi", "parallel_calig"]
+    plugins = C5_PLUGINS
     t0 = time.perf_counter()
     own = Engine(plugins[0], max_results=cfg["max_results"], max_batch=B, deadline_ns=cfg["deadline_ns"],
-                 graphs=True)
+                 graphs=True, device=device)
     qv0, qe0 = w.queries[0]
     own.set_query(qv0, qe0)
     vls = np.concatenate([q[0] for q in w.queries])
@@ -437,19 +451,25 @@ def run_stress_config(args, cfg):
     own.build_index()
     att = [own.attach(*w.queries[i], plugins[i % len(plugins)], max_results=cfg["max_results"])
            for i in range(1, len(w.queries))]
-    log(f"engine with {len(w.queries)} queries ready in {time.perf_counter() - t0:.1f}s")
+    log(f"C5 engine with {len(w.queries)} queries ready in {time.perf_counter() - t0:.1f}s")
     for i in range(W):
         own.run(w.stream[i * B:(i + 1) * B])
-    t1 = time.perf_counter()
+    ext = torch.cuda.ExternalStream(own.stream(), device=f"cuda:{device}")
     res = [[] for _ in range(len(w.queries))]
+    ms = 0.0
     for k in range(K):
-        chunk = w.stream[(W + k) * B:(W + k + 1) * B]
+        chunk = np.ascontiguousarray(w.stream[(W + k) * B:(W + k + 1) * B])
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(ext)
         first = own.submit(chunk)
+        b.record(ext)
+        b.synchronize()
+        ms += a.elapsed_time(b)
         own.wait()
         res[0].append(own.results(first, len(chunk)))
-        for i, a in enumerate(att):
-            res[i + 1].append(a.results(first, len(chunk)))
-    secs = time.perf_counter() - t1
+        for i, q in enumerate(att):
+            res[i + 1].append(q.results(first, len(chunk)))
     per_q = []
     for i, rs in enumerate(res):
         r = np.concatenate(rs)
@@ -462,12 +482,28 @@ def run_stress_config(args, cfg):
                       "p99_us": float(np.percentile(r["latency_ns"], 99)) / 1e3})
     allr = np.concatenate([np.concatenate(rs) for rs in res])
     bad = (allr["status"] == ST_CAPPED) | (allr["status"] == ST_TIMED_OUT)
-    line = {"metric": METRIC, "value": K * B / secs, "unit": "updates/s", "n_gpus": 1, "steps": K, "warmup": W,
-            "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "batch": B, "max_results": cfg["max_results"],
-                       "deadline_ns": cfg["deadline_ns"], "timing": "host wall clock around submit + results"},
-            "success_rate": float(1 - bad.mean()), "queries": per_q}
+    for q in att:
+        q.close()
+    own.close()
+    return {"workload": cfg["workload"], "batch": B, "warmup_batches": W, "timed_batches": K,
+            "max_results": cfg["max_results"], "deadline_ns": cfg["deadline_ns"],
+            "updates_per_s": K * B / (ms / 1e3) if ms > 0 else None, "ms_per_batch": ms / K if K else None,
+            "success_rate": float(1 - bad.mean()), "queries": per_q,
+            "timing": "CUDA events on the owner's stream around each submit (all four queries' searches)"}
+
+
+def run_stress_config(args, cfg):
+    """C5 on its own: value = updates/s over the timed batches."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    leg = c5_leg(args.warmup, args.steps)
+    line = {"metric": METRIC, "value": leg["updates_per_s"], "unit": "updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": leg["ms_per_batch"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "batch": cfg["batch"], "max_results": cfg["max_results"],
+                       "deadline_ns": cfg["deadline_ns"]},
+            "success_rate": leg["success_rate"], "c5": leg}
     print(json.dumps(line), flush=True)
 
 
@@ -493,6 +529,11 @@ def main():
     ap.add_argument("--serve-rates", default="1e4,1e5,1e6",
                     help="offered loads (updates/s) for the serving-loop leg; empty to skip")
     ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--extra-configs", default="c4,c5",
+                    help="bounded legs of the other configs added to the default line (c4: 64 standing queries "
+                         "served over a rate sweep; c5: large queries with the CaLiG- and NewSP-style plugins); "
+                         "empty to skip")
+    ap.add_argument("--c4-seconds", type=float, default=8.0, help="seconds of arrivals per offered rate (C4 leg)")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.algo:
@@ -707,6 +748,18 @@ def main():
         log(f"parity against the reference SymBi: {parity['updates_compared']} updates, "
             f"{parity['mismatches']} mismatches")
 
+    # ---- bounded legs of the serving (C4) and large-query (C5) configs ----
+    extra = {}
+    extras = [x for x in args.extra_configs.split(",") if x] if (rank == 0 and world == 1) else []
+    if "c4" in extras:
+        t1 = time.perf_counter()
+        extra["c4"] = c4_leg([1e4, 1e5, 1e6], args.c4_seconds, device=dev)
+        extra["c4"]["wall_s"] = time.perf_counter() - t1
+    if "c5" in extras:
+        t1 = time.perf_counter()
+        extra["c5"] = c5_leg(1, 2, device=dev)
+        extra["c5"]["wall_s"] = time.perf_counter() - t1
+
     if rank == 0:
         clocks = clk.summary()
         line = {
@@ -733,6 +786,7 @@ def main():
             "cpu_baseline": cpu,
             "cpu_baseline_sequential_symbi_capped": cpu_seq,
             "parity": parity,
+            **extra,
             "gpu_launches": launches,
             "clocks": clocks,
             "counts": {"positive": int(res["pos"].sum()), "negative": int(res["neg"].sum()),

@@ -3,7 +3,7 @@
 //   csm_serve -w WORKLOAD_DIR [--queries N] [--rate R] [--max-batch B] [--budget-gb G]
 //             [--cap N] [--plugins symbi,turboflux,graphflow,calig,newsp] [--arrive-every S]
 //             [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]
-//             [--deadline-ms MS] [--device D]
+//             [--deadline-ms MS] [--device D] [--rates R1,R2,...]
 //             [--out results.bin]
 //   csm_serve -d data -u stream -q query[:plugin[:cap[:arrive_s]]] [-q ...] [same options]
 //
@@ -11,6 +11,10 @@
 // query_<i>.graph); its queries get the plugins round-robin.  Prints one JSON
 // line with the offered rate, sustained updates/s, p50 / p99 per-update
 // latency (arrival to results on the host), batches and admitted queries.
+// --rates sweeps offered loads in one run: --max-seconds of arrivals per
+// rate, each segment continuing the stream and the graph where the last one
+// stopped; one JSON line per segment ("segment": i) precedes the line of the
+// whole run.
 // --out writes every admitted query's per-update results:
 //   "CSMR", u32 n_queries, then per query: u32 admitted, u64 first, u64 count,
 //   count x csm_result (48 bytes).
@@ -54,7 +58,7 @@ void usage() {
           "csm_serve -w DIR | -d data -u stream -q query[:plugin[:cap[:arrive_s]]]...\n"
           "  [--queries N] [--rate R] [--max-batch B] [--budget-gb G] [--cap N] [--plugins a,b,c]\n"
           "  [--arrive-every S] [--max-updates N] [--max-seconds S] [--seed S] [--hash 0|1] [--graphs 0|1]\n"
-          "  [--deadline-ms MS] [--device D]\n"
+          "  [--deadline-ms MS] [--device D] [--rates R1,R2,...]\n"
           "  [--out results.bin]\n");
 }
 
@@ -93,6 +97,10 @@ int main(int argc, char** argv) {
       else if (k == "--graphs") cfg.graphs = std::stoi(val()) != 0;
       else if (k == "--deadline-ms") cfg.deadline_ns = (uint64_t)(std::stod(val()) * 1e6);
       else if (k == "--device") cfg.device = std::stoi(val());
+      else if (k == "--rates") {
+        for (const std::string& r : split(val(), ','))
+          if (!r.empty()) cfg.rates.push_back(std::stod(r));
+      }
       else if (k == "--out") out_path = val();
       else if (k == "-h" || k == "--help") { usage(); return 0; }
       else { fprintf(stderr, "unknown option %s\n", k.c_str()); usage(); return 2; }
@@ -139,10 +147,24 @@ int main(int argc, char** argv) {
   }
   std::vector<ServeQueryResult> res;
   ServeStats st;
-  int rc = serve(data, stream, queries, cfg, res, st, err);
+  std::vector<ServeStats> sweep;
+  int rc = serve(data, stream, queries, cfg, res, st, err, &sweep);
   if (rc) {
     fprintf(stderr, "serve failed (%d): %s\n", rc, err.c_str());
     return 1;
+  }
+  if (!cfg.rates.empty()) {
+    for (size_t i = 0; i < sweep.size(); i++) {
+      const ServeStats& x = sweep[i];
+      printf("{\"segment\": %zu, \"offered_rate\": %.1f, \"sustained\": %.1f, \"updates\": %llu, "
+             "\"elapsed_s\": %.4f, \"p50_us\": %.1f, \"p99_us\": %.1f, \"batches\": %llu, \"mean_batch\": %.1f, "
+             "\"max_batch_seen\": %llu, \"queries_admitted\": %u, \"queries_refused\": %u, "
+             "\"device_bytes\": %llu, \"success_rate\": %.6f}\n",
+             i, cfg.rates[i], x.sustained, (unsigned long long)x.updates, x.elapsed_s, x.p50_us, x.p99_us,
+             (unsigned long long)x.batches, x.mean_batch, (unsigned long long)x.max_batch_seen, x.queries_admitted,
+             x.queries_refused, (unsigned long long)x.device_bytes,
+             x.results ? 1.0 - (double)x.incomplete / (double)x.results : 1.0);
+    }
   }
   uint64_t pos = 0, neg = 0, capped = 0;
   for (const ServeQueryResult& r : res)

@@ -44,6 +44,9 @@ struct ServeConfig {
   bool graphs = true;                    // replay each batch size's launch sequence as a CUDA graph
   uint64_t deadline_ns = 0;              // per-update search time limit (0: none)
   double max_seconds = 0;                // stop admitting updates after this long (0: run the stream)
+  // offered loads of a sweep: one segment of max_seconds per rate, one after
+  // another on the same graph, queries and stream (empty: `rate` alone)
+  std::vector<double> rates;
 };
 
 struct ServeQueryResult {
@@ -62,8 +65,11 @@ struct ServeStats {
 };
 
 // Runs the stream through the serving loop.  Returns CSM_OK or a CSM_E* code
-// (text in csm_gpu_last_error() or `err`).
+// (text in csm_gpu_last_error() or `err`).  With cfg.rates, `sweep` receives
+// one ServeStats per rate (each segment continues the stream where the last
+// one stopped) and `stats` covers the whole run.
 int serve(const EdgeList& data, const std::vector<Update>& stream, const std::vector<ServeQuery>& queries,
-          const ServeConfig& cfg, std::vector<ServeQueryResult>& out, ServeStats& stats, std::string& err);
+          const ServeConfig& cfg, std::vector<ServeQueryResult>& out, ServeStats& stats, std::string& err,
+          std::vector<ServeStats>* sweep = nullptr);
 
 }  // namespace csm
