@@ -19,6 +19,15 @@ before the stream.
     python tests/golden/make_golden.py --initial  # only initial.json (InitialMatching counts of csm)
     python tests/golden/make_golden.py --calig    # only the calig_* cases
     python tests/golden/make_golden.py --c3shape  # only the c3_shape case
+    python tests/golden/make_golden.py --selfloop # only the selfloop case
+
+The selfloop case is a data graph with self loops (the generator never
+writes them; the reference's Graph::AddEdge stores a loop's vertex twice in
+its own neighbour list, ParaCOSM/CSM/graph/graph.cpp:58-76) and a query with
+an edge between two vertices of one label, so that under --homo an embedding
+can map that edge onto a loop.  selfloop.csv holds sequential SymBi's
+per-update counts with and without --homo, on the graph with its loops and
+on the same graph without them.
 
 The c3_shape case has the shape of the 2^22-vertex SymBi benchmark at a size
 the CPU finishes: 2^16 vertices, average degree 28, 16 vertex labels
@@ -196,7 +205,49 @@ def write_c3_shape() -> None:
     print("c3_shape updates", n, "nonzero", sum(1 for i in range(n) if full[i]["pos"] or full[i]["neg"]))
 
 
+SELFLOOP = ["--preset", "c2", "--log2-n", "10", "--avg-degree", "8", "--vlabels", "2", "--zipf", "0",
+            "--elabels", "1", "--updates", "300", "--insert-frac", "0.8", "--seed", "17", "--query", "4:dense"]
+
+
+def write_selfloop() -> None:
+    import random
+
+    d = HERE / "selfloop"
+    tmp = HERE / "_tmp_selfloop"
+    if tmp.exists():
+        shutil.rmtree(tmp)
+    subprocess.run([str(GEN)] + SELFLOOP + ["--out", str(tmp), "--text"], check=True, capture_output=True)
+    d.mkdir(exist_ok=True)
+    lines = (tmp / "data.graph").read_text().splitlines()
+    n = sum(1 for x in lines if x.startswith("v "))
+    rng = random.Random(17)
+    loops = [f"e {v} {v} 0" for v in sorted(rng.sample(range(n), 80))]
+    (d / "data.graph").write_text("\n".join(lines + loops) + "\n")
+    (d / "data_noloop.graph").write_text("\n".join(lines) + "\n")
+    shutil.copy(tmp / "stream.txt", d / "stream.txt")
+    shutil.copy(tmp / "query_0.graph", d / "query.graph")
+    shutil.rmtree(tmp)
+    cols = {}
+    for name, data, homo in (("loop", "data.graph", False), ("loop_homo", "data.graph", True),
+                             ("noloop_homo", "data_noloop.graph", True)):
+        rows, _ = pyoracle.ref_run(d / "query.graph", d / data, d / "stream.txt", "symbi", homo=homo, timeout=600)
+        cols[name] = rows
+    with open(d / "selfloop.csv", "w") as f:
+        f.write("idx,pos,neg,homo_pos,homo_neg,homo_noloop_pos,homo_noloop_neg\n")
+        for i in range(len(cols["loop"])):
+            a, b, c = cols["loop"][i], cols["loop_homo"][i], cols["noloop_homo"][i]
+            f.write(f"{i},{a['pos']},{a['neg']},{b['pos']},{b['neg']},{c['pos']},{c['neg']}\n")
+    (d / "params.json").write_text(json.dumps({"generator": SELFLOOP, "self_loops": 80, "label": 0,
+                                               "reference": "ParaCOSM/CSM/matching/SymBi (sequential)"}, indent=1) + "\n")
+    diff = sum(1 for i in range(len(cols["loop"])) if cols["loop_homo"][i]["pos"] != cols["noloop_homo"][i]["pos"]
+               or cols["loop_homo"][i]["neg"] != cols["noloop_homo"][i]["neg"])
+    print("selfloop updates", len(cols["loop"]), "homo counts changed by the loops at", diff, "updates")
+
+
 def main() -> None:
+    if "--selfloop" in sys.argv:
+        write_selfloop()
+        return
     if "--c3shape" in sys.argv:
         write_c3_shape()
         return

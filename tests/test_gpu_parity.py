@@ -312,3 +312,23 @@ def test_plain_form_launches_per_update(algo):
             if algo != "parallel_calig":
                 assert (int(r["pos"]), int(r["neg"])) == (int(x["symbi_pos"][i]), int(x["symbi_neg"][i])), i
         assert seen[True] > 20 and seen[False] > 20
+
+
+@pytest.mark.parametrize("homo", [False, True])
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_self_loops_in_the_data_graph(homo, mode):
+    """The engine drops data self loops at load: without --homo its counts equal the reference
+    SymBi's on the graph with loops, with --homo the reference's on the same graph without them
+    (the reference's --homo counts with loops differ; see the self-loop fixture)."""
+    import csv
+
+    from conftest import GOLDEN
+    d = GOLDEN / "selfloop"
+    qv, qe = workload.read_graph(d / "query.graph")
+    vl, e = workload.read_graph(d / "data.graph")
+    s = workload.read_stream(d / "stream.txt")
+    rows = list(csv.DictReader(open(d / "selfloop.csv")))
+    x = {k: np.array([int(r[k]) for r in rows], dtype=np.uint64) for k in rows[0] if k != "idx"}
+    res, _ = run_engine(qv, qe, vl, e, s, "parallel_symbi", homo=homo, mode=mode, want_hash=False)
+    pos, neg = (x["homo_noloop_pos"], x["homo_noloop_neg"]) if homo else (x["pos"], x["neg"])
+    assert_same(res, pos, neg)
