@@ -524,6 +524,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
   const unsigned long long t_start = global_ns();
   constexpr bool EN = MODE == 1;
   const int tail_level = (MODE == 2 && p.tail && A->tail_at) ? (int)A->tail_at : -1;
+  uint32_t seen_stop = 0, seen_hungry = 0;  // lane 0: flags loaded in the previous iteration
   while (d >= 1) {
     ++iter;
     if ((iter & 63) == 0 && p.deadline_ns) {
@@ -554,15 +555,20 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       }
     }
     if ((iter & 7) == 0) {
-      uint32_t st = (lane == 0) ? stop[t] : 0u;
-      if (__shfl_sync(0xffffffffu, st, 0)) break;
+      if (__shfl_sync(0xffffffffu, seen_stop, 0)) break;
     }
     if ((iter & (p.donate_every ? p.donate_every - 1 : 3u)) == 0 && p.dq) {
-      uint32_t idle_now = (lane == 0) ? *(volatile unsigned int*)&p.q->hungry : 0u;
-      idle_now = __shfl_sync(0xffffffffu, idle_now, 0);
+      const uint32_t idle_now = __shfl_sync(0xffffffffu, seen_hungry, 0);
       acc.checks++;
       if (idle_now) acc.checks_hungry++;
       if (idle_now) donate(p, lv, d, lane, idle_now, t, T, m0, m1, tail_level);
+    }
+    // the stop flag and the idle-warp count the checks above read are loaded
+    // one iteration ahead, so their round trip to L2 overlaps a step's work
+    // instead of preceding it (a step late is soon enough for both)
+    if (lane == 0) {
+      seen_stop = stop[t];
+      seen_hungry = p.dq ? *(volatile unsigned int*)&p.q->hungry : 0u;
     }
     if constexpr (MODE == 2) {
       if (d == tail_level) {
