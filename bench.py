@@ -187,7 +187,10 @@ class RefRun:
     overlap.  A watchdog ends a run `budget` seconds into its update loop, even inside an update
     (parallel TurboFlux ignores the result cap below depth 2)."""
 
-    def __init__(self, w, algo: str, threads: int, cap: int, first: int, budget: float, gated: bool, tag: str):
+    def __init__(self, w, algo: str, threads: int, cap: int, first: int, budget: float, gated: bool, tag: str,
+                 apply: bool = False):
+        """apply: start from the initial graph and let the reference's Graph apply the first `first`
+        updates itself (--apply-to) instead of loading the generator's snapshot there."""
         self.algo, self.threads, self.first, self.budget = algo, threads, first, budget
         self.tmp = Path(tempfile.mkdtemp(prefix=f"csm_ref_{tag}_"))
         self.out = self.tmp / "rows.csv"
@@ -198,10 +201,10 @@ class RefRun:
         if not drv.exists():
             self.err = "reference driver not built (oracle/_ref/ref_driver)"
             return
-        graph = w.directory / (f"data_at_{first}.bin" if first else "data.bin")
+        graph = w.directory / (f"data_at_{first}.bin" if first and not apply else "data.bin")
+        start = ["--apply-to", str(first)] if apply and first else ["--first", str(first)]
         cmd = [str(drv), "-q", str(w.query_path(0)), "-D", str(graph), "-U", str(w.directory / "stream.bin"),
-               "-a", algo, "-t", str(threads), "--first", str(first), "--wall-budget", str(budget),
-               "--out", str(self.out)]
+               "-a", algo, "-t", str(threads)] + start + ["--wall-budget", str(budget), "--out", str(self.out)]
         if cap:
             cmd += ["--max-results", str(cap)]
         if gated:
@@ -311,6 +314,22 @@ def run_timed_refs(refs: list[RefRun], cfg, budget: float) -> list[dict]:
             r.kill()
         out.append(cpu_line(r, res, cfg))
     return out
+
+
+def start_parity_refs(w, cfg, end: int, budget: float) -> list[RefRun]:
+    """Sequential SymBi (the reference plugin that stops at exactly max_results, as the engine does)
+    on several segments of the stream [0, end) at once, each starting where its segment begins
+    (the reference's Graph applies the earlier updates itself): one run gets stuck on the rare
+    update whose search takes minutes, the others keep comparing.  As many runs as host cores
+    and memory allow (a run holds about 9 GB at 2^22 vertices), at most 12."""
+    try:
+        import psutil
+        mem_gb = psutil.virtual_memory().available / 2**30
+    except Exception:
+        mem_gb = 64.0
+    n = int(max(1, min(12, (os.cpu_count() or 2) - 2, (mem_gb - 40) // 10)))
+    return [RefRun(w, "symbi", 1, cfg["max_results"], (k * end // n) // 1000 * 1000, budget, True, f"par{k}",
+                   apply=True) for k in range(n)]
 
 
 def parity_check(rows: np.ndarray, gpu: np.ndarray, base: int, cap: int) -> dict:
@@ -571,10 +590,10 @@ def main():
     # ---- the reference on the host cores (rank 0, one GPU): the timed runs load now and
     # start their update loops after the GPU legs; the parity run (sequential SymBi from the
     # initial graph, the warm-up batches' updates) runs meanwhile ----
-    cpu_refs, par_ref = [], None
+    cpu_refs, par_refs = [], []
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu_refs = start_timed_refs(w, cfg, first, args.cpu_budget)
-        par_ref = RefRun(w, "symbi", 1, cfg["max_results"], 0, args.parity_budget, False, "parity")
+        par_refs = start_parity_refs(w, cfg, (W + K) * B, args.parity_budget)
 
     # ---- batched engine, inputs resident in HBM ----
     t0 = time.perf_counter()
@@ -731,12 +750,18 @@ def main():
 
     # ---- the reference: parity of the counts, then the timed runs one after another ----
     cpu, cpu_seq, parity, checks = None, None, None, {}
-    if par_ref is not None:
-        par_ref.collect(args.parity_budget + 3600)
-        rows = par_ref.rows()
-        checks = {"from_initial_graph": parity_check(rows, warm_res, 0, cfg["max_results"])}
-        parity = {"reference": "symbi -t 1 (reference sources, sequential update order, cap-honouring)",
-                  "engine": "batched warm-up batches, then the timed window"}
+    if par_refs:
+        # the engine's results for updates [0, (W + K) * B): warm-up batches, then the timed window
+        gpu_all = np.concatenate([warm_res, res])
+        for r in par_refs:
+            if r.wait_ready(3600):
+                r.go()
+        for k, r in enumerate(par_refs):
+            r.collect(args.parity_budget + 600)
+            checks[f"segment_{k}"] = parity_check(r.rows(), gpu_all, 0, cfg["max_results"])
+        parity = {"reference": "symbi -t 1 (reference sources, sequential update order, cap-honouring), "
+                               f"{len(par_refs)} runs on segments of the stream, {args.parity_budget:.0f}s each",
+                  "engine": "batched: the warm-up batches and the timed window"}
     if cpu_refs:
         cpu, cpu_seq = run_timed_refs(cpu_refs, cfg, args.cpu_budget)
         # the sequential SymBi run times the first updates of the timed window: its counts too

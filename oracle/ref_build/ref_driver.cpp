@@ -118,6 +118,7 @@ struct Args {
   std::vector<long> dump_at;  // update counts after which the index is dumped (0: after preprocessing)
   size_t threads = 1, auto_tuning = 0, max_updates = SIZE_MAX;
   size_t first = 0;         // index of the first stream update to run (the data graph is the state there)
+  size_t apply_to = 0;      // apply stream updates [0, N) to the data graph itself, then start at N
   uint64_t max_results = UINT32_MAX;
   double time_budget = 0;   // stop after the update that crosses this many seconds
   double wall_budget = 0;   // hard limit: report and exit even inside an update
@@ -176,6 +177,8 @@ void usage() {
           "  [-t threads] [--auto-tuning 0|1] [--max-results N] [--homo 0|1]\n"
           "  [--hash] [--out per_update.csv] [--max-updates N] [--time-budget S] [--wall-budget S]\n"
           "  [--first N]   (start at stream update N; give the data graph as it stands there)\n"
+          "  [--apply-to N] (apply stream updates [0, N) to the data graph with Graph::AddEdge /\n"
+          "                 RemoveEdge before preprocessing, then start at update N)\n"
           "  [--gate PATH] (after preprocessing write PATH.ready; start the updates once PATH.go exists)\n"
           "  [--dump-index FILE --dump-at N,N,...]   (symbi / turboflux: root, DAG, d1 / d2 flags)\n");
 }
@@ -201,6 +204,7 @@ int main(int argc, char** argv) {
     else if (k == "--out") a.out = nxt();
     else if (k == "--max-updates") a.max_updates = std::stoull(nxt());
     else if (k == "--first") a.first = std::stoull(nxt());
+    else if (k == "--apply-to") a.apply_to = std::stoull(nxt());
     else if (k == "--gate") a.gate = nxt();
     else if (k == "--time-budget") a.time_budget = std::stod(nxt());
     else if (k == "--wall-budget") a.wall_budget = std::stod(nxt());
@@ -243,11 +247,29 @@ int main(int argc, char** argv) {
 
   EnumHashBuf hb(query.NumVertices());
   std::streambuf* old = nullptr;
+  auto load_stream = [&]() -> bool {
+    if (!a.ubin.empty()) return read_binary_stream(a.ubin, data);
+    data.LoadUpdateStream(a.u);
+    return true;
+  };
+  if (a.apply_to) {
+    // the graph as it stands after the stream's first updates, built by the
+    // reference's own Graph methods (no plugin sees these updates)
+    if (!load_stream()) { fprintf(stderr, "bad stream\n"); return 1; }
+    const size_t na = std::min(a.apply_to, data.updates_vec_.size());
+    for (size_t i = 0; i < na; i++) {
+      const InsertUnit& up = data.updates_vec_[i];
+      if (up.type == 'v' && up.is_add) data.AddVertex(up.id1, up.label);
+      else if (up.type == 'v') data.RemoveVertex(up.id1);
+      else if (up.is_add) data.AddEdge(up.id1, up.id2, up.label);
+      else data.RemoveEdge(up.id1, up.id2);
+    }
+    a.first = na;
+  }
   mm->Preprocessing();
   auto t2 = std::chrono::steady_clock::now();
 
-  if (!a.ubin.empty()) { if (!read_binary_stream(a.ubin, data)) { fprintf(stderr, "bad stream %s\n", a.ubin.c_str()); return 1; } }
-  else data.LoadUpdateStream(a.u);
+  if (!a.apply_to && !load_stream()) { fprintf(stderr, "bad stream\n"); return 1; }
   // --first N: the data graph given is the state after updates [0, N), and the
   // loop runs updates N, N + 1, ... in order (rows keep their stream index)
   const size_t first = std::min(a.first, data.updates_vec_.size());
