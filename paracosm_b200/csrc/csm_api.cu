@@ -78,6 +78,9 @@ struct csm_ctx {
   bool has_graph = false;
   DevGraph g{};
   std::vector<uint32_t> h_vlabel;  // folded vertex labels (kNone: no vertex), mirrored on the host
+  // edge table (DevGraph::ekeys): upper bounds of its live keys and deleted
+  // slots, from the updates submitted since it was last filled
+  uint64_t e_live = 0, e_tomb = 0;
   uint64_t num_edges = 0;
   // candidate index
   IndexState index{};
@@ -421,6 +424,7 @@ static int batch_mutate_insert(csm_ctx* ctx, const csm_update* ups, uint32_t B, 
   launch_mut_insert(ctx->d_rins, c + 3, ctx->d_ins2, ctx->d_ins_dst, g, mut_blocks, (uint32_t)ctx->sm_count * 2, st);
   CKL();
   ctx->launches++;
+  if (g.emask) { k_edge_list<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_ins2, L, g, 0u); CKL(); }
   return CSM_OK;
 }
 
@@ -548,6 +552,7 @@ static int run_edge_batch(csm_ctx* ctx, const csm_update* ups, uint32_t B, csm_r
   launch_mut_delete(ctx->d_rdel, c + 4, ctx->d_del2, ctx->d_ins_dst, g, mut_blocks, (uint32_t)ctx->sm_count * 2, st);
   CKL();
   ctx->launches++;
+  if (g.emask) { k_edge_list<<<blocks_for(L, 256), 256, 0, st>>>(ctx->d_del2, L, g, 1u); CKL(); }
   for (csm_ctx* a : ctx->attached) {
     rc = stream_after(a->st, st, ctx->ev_fork);
     if (!rc) rc = index_apply_edges(a->index, g, ctx->d_del2, L, a->st, &a->launches);
@@ -673,6 +678,8 @@ static int run_vertex_delete(csm_ctx* ctx, uint32_t v) {
                       st);
     CKL();
     ctx->launches++;
+    if (g.emask) { k_edge_list<<<blocks_for(K, 256), 256, 0, st>>>(keys2, K, g, 1u); CKL(); }
+    ctx->e_tomb += deg;
     for (csm_ctx* q : all) {
       if (q != ctx) { q->g = g; rc = stream_after(q->st, st, ctx->ev_fork); }
       if (!rc) rc = index_apply_edges(q->index, g, keys2, K, q->st, &q->launches);
@@ -796,6 +803,46 @@ static int run_edge_batch_graph(csm_ctx* ctx, const csm_update* ups, uint32_t B_
   return CSM_OK;
 }
 
+// Keeps the edge table's load below one half (live keys plus deleted slots)
+// before the updates `h` of a submit run: refills it from the CSR when the
+// deleted slots would push it over, in a table twice as large when the live
+// keys alone fill a third.  The counts are upper bounds (every insertion
+// record counts as a new edge, every deletion as a deleted slot).
+static int edge_table_maintain(csm_ctx* ctx, const csm_update* h, uint64_t n) {
+  DevGraph& g = ctx->g;
+  if (!g.emask) return CSM_OK;
+  uint64_t ins = 0, del = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    if (h[i].type != 'e') continue;
+    if (h[i].is_add) ins++; else del++;
+  }
+  uint64_t slots = g.emask + 1;
+  if ((ctx->e_live + ctx->e_tomb + ins + del) * 2 > slots) {
+    cudaStream_t st = ctx->st;
+    uint64_t want = slots;
+    while ((ctx->e_live + ins) * 3 > want) want <<= 1;
+    if (want != slots) {
+      uint64_t* nk = nullptr;
+      CK(cudaStreamSynchronize(st));  // no kernel of an earlier submit still reads the old table
+      for (csm_ctx* a : ctx->attached) CK(cudaStreamSynchronize(a->st));
+      int rc = ctx->mem.alloc((void**)&nk, 8ull * want);
+      if (rc) return rc;
+      ctx->mem.release(g.ekeys, 8ull * slots);
+      g.ekeys = nk;
+      g.emask = want - 1;
+      slots = want;
+      ctx->graph_version++;  // captured launch sequences hold the old table
+    }
+    CK(cudaMemsetAsync(g.ekeys, 0xff, 8ull * slots, st));
+    k_edge_fill<<<ctx->sm_count * 8, 256, 0, st>>>(g);
+    CKL();
+    ctx->e_tomb = 0;
+  }
+  ctx->e_live += ins;
+  ctx->e_tomb += del;
+  return CSM_OK;
+}
+
 static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, const csm_update* h_ups) {
   if (ctx->owner) return set_err(CSM_ESTATE, "updates of an attached query are submitted to its owner");
   if (!ctx->has_graph || !ctx->has_plan) return set_err(CSM_ESTATE, "load the query, the graph and build the index first");
@@ -830,6 +877,8 @@ static int submit_common(csm_ctx* ctx, uint64_t n, const csm_update* d_ups, cons
     CK(cudaStreamSynchronize(st));
     h = hv.data();
   }
+  rc = edge_table_maintain(ctx, h, n);
+  if (rc) return rc;
   uint64_t i = 0;
   while (i < n) {
     for (size_t k = 0; k < ctx->attached.size(); k++) out_q[k] = ctx->attached[k]->d_results + i;
@@ -898,7 +947,7 @@ static int check_device_error(csm_ctx* ctx) {
   if (ps.error) {
     static const char* names[] = {"none", "row pool exhausted", "batch list overflow", "task list overflow",
                                   "search queue wait limit", "malformed donated task", "ring left undrained",
-                                  "task time guard", "row state"};
+                                  "task time guard", "row state", "edge table full"};
     char extra[256] = "";
     if (ctx->d_sstat) {
       SearchStats ss;
@@ -921,7 +970,7 @@ static int check_device_error(csm_ctx* ctx) {
     ps.error = 0;
     cudaMemcpy(ctx->g.ps, &ps, sizeof(PoolState), cudaMemcpyHostToDevice);
     reset_ring(ctx);
-    return set_err(CSM_EDEVICE, "device error %u (%s)%s", code, code < 9 ? names[code] : "?", extra);
+    return set_err(CSM_EDEVICE, "device error %u (%s)%s", code, code < 10 ? names[code] : "?", extra);
   }
   return CSM_OK;
 }
@@ -1525,6 +1574,28 @@ int csm_gpu_load_graph(csm_ctx* ctx, uint32_t n_v, const uint32_t* vlabels, uint
   m.release(tmp, tbmax); m.release(d_small, 64);
 #undef AL
   ctx->num_edges = n_valid / 2;
+  // edge table: four slots per edge (a power of two); without room for it,
+  // or for ids of 30 bits and more or over 16 folded edge labels, the
+  // search joins by binary search in the rows instead
+  g.ekeys = nullptr;
+  g.emask = 0;
+  if (n_cap < (1u << 30) && n_el <= 16) {
+    uint64_t slots = 1ull << 20;
+    while (slots < 4 * std::max<uint64_t>(ctx->num_edges, 1)) slots <<= 1;
+    uint64_t* ek = nullptr;
+    if (m.alloc((void**)&ek, 8ull * slots) == CSM_OK) {
+      g.ekeys = ek;
+      g.emask = slots - 1;
+      CK(cudaMemsetAsync(g.ekeys, 0xff, 8ull * slots, st));
+      k_edge_fill<<<ctx->sm_count * 8, 256, 0, st>>>(g);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(st));
+      ctx->e_live = ctx->num_edges;
+      ctx->e_tomb = 0;
+    } else {
+      set_err(CSM_OK, "");  // the table is optional
+    }
+  }
   ctx->has_graph = true;
   return CSM_OK;
 }

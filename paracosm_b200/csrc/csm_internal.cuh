@@ -71,7 +71,7 @@ struct PoolState {
   uint32_t pad;
 };
 enum : uint32_t { kErrNone = 0, kErrPoolFull = 1, kErrListOverflow = 2, kErrTaskOverflow = 3, kErrWaitTimeout = 4,
-                  kErrBadTask = 5, kErrRingState = 6, kErrTaskGuard = 7, kErrRowState = 8 };
+                  kErrBadTask = 5, kErrRingState = 6, kErrTaskGuard = 7, kErrRowState = 8, kErrEdgeTable = 9 };
 
 // Device view of the dynamic CSR (pointers into device memory).
 struct DevGraph {
@@ -94,7 +94,40 @@ struct DevGraph {
   uint32_t n_qv, n_qe;
   uint32_t n, n_cap, n_vl, n_el, nc;  // n_vl = n_qv + 1, n_el = n_qe + 1
   KeyBits kb;
+  // Edge table: every (edge, label) of the graph -- the union graph during a
+  // batch -- as one key in an open-addressing hash set (linear probing), so
+  // that "is x a neighbour of v over label l" is one probe instead of a
+  // binary search in v's segment.  emask = slots - 1; 0: no table (ids of
+  // 30 bits or more, or more than 16 folded edge labels).
+  uint64_t* ekeys;
+  uint64_t emask;
 };
+
+// Edge-table keys: the smaller endpoint (30 bits), the larger (30 bits), the
+// folded edge label (4 bits); two values no key takes mark empty and deleted
+// slots.
+constexpr uint64_t kEdgeEmpty = ~0ULL, kEdgeTomb = ~0ULL - 1;
+__host__ __device__ __forceinline__ uint64_t edge_key(uint32_t a, uint32_t b, uint32_t l) {
+  const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  return ((uint64_t)lo << 34) | ((uint64_t)hi << 4) | (uint64_t)l;
+}
+__device__ __forceinline__ uint64_t edge_slot(uint64_t key, uint64_t mask) {
+  uint64_t x = key ^ (key >> 33);  // MurmurHash3 fmix64, as mix64
+  x *= 0xff51afd7ed558ccdULL; x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+  return x & mask;
+}
+// Probe sequence from a slot already loaded (first = ekeys[slot]).
+__device__ __forceinline__ bool edge_probe_rest(const DevGraph& g, uint64_t key, uint64_t slot, uint64_t first) {
+  uint64_t k = first;
+  for (uint64_t n = 0; n <= g.emask; n++) {
+    if (k == key) return true;
+    if (k == kEdgeEmpty) return false;
+    slot = (slot + 1) & g.emask;
+    k = g.ekeys[slot];
+  }
+  return false;
+}
 
 __device__ __forceinline__ uint32_t fold_label(const uint32_t* sorted, uint32_t n, uint32_t l) {
   uint32_t lo = 0, hi = n;

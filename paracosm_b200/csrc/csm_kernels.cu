@@ -494,6 +494,66 @@ void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const
   k_mut_delete_g<256><<<big_blocks, 256, 0, st>>>(ranges, n_ranges, del_key, del_pos, g);
 }
 
+// ------------------------------------------------------------ edge table
+
+__device__ __forceinline__ void edge_insert(const DevGraph& g, uint64_t key) {
+  uint64_t slot = edge_slot(key, g.emask);
+  for (uint64_t n = 0; n <= g.emask; n++) {
+    const uint64_t k = g.ekeys[slot];
+    if (k == key) return;
+    if (k == kEdgeEmpty) {
+      const unsigned long long prev =
+          atomicCAS((unsigned long long*)&g.ekeys[slot], (unsigned long long)kEdgeEmpty, (unsigned long long)key);
+      if (prev == kEdgeEmpty || prev == key) return;  // placed here, or by another thread inserting the same key
+    }
+    slot = (slot + 1) & g.emask;
+  }
+  atomicExch(&g.ps->error, kErrEdgeTable);  // no empty slot left
+}
+
+__device__ __forceinline__ void edge_delete(const DevGraph& g, uint64_t key) {
+  uint64_t slot = edge_slot(key, g.emask);
+  for (uint64_t n = 0; n <= g.emask; n++) {
+    const uint64_t k = g.ekeys[slot];
+    if (k == key) {
+      atomicCAS((unsigned long long*)&g.ekeys[slot], (unsigned long long)key, (unsigned long long)kEdgeTomb);
+      return;
+    }
+    if (k == kEdgeEmpty) return;
+    slot = (slot + 1) & g.emask;
+  }
+}
+
+__global__ void k_edge_fill(DevGraph g) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t* pool = g.pools[g.ps->active];
+  for (uint32_t v = warp; v < g.n; v += nwarps) {
+    const uint32_t* dirv = g.dir + (size_t)v * (g.nc + 1);
+    if (dirv[g.nc] == 0) continue;
+    const uint64_t off = g.row_off[v];
+    for (uint32_t c = 0; c < g.nc; c++) {
+      const uint32_t lo = dirv[c], hi = dirv[c + 1];
+      for (uint32_t i = lo + lane; i < hi; i += 32) {
+        const uint32_t w = pool[off + i];
+        if (v < w) edge_insert(g, edge_key(v, w, c % g.n_el));
+      }
+    }
+  }
+}
+
+__global__ void k_edge_list(const uint64_t* keys, uint32_t L, DevGraph g, uint32_t del) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L) return;
+  const uint64_t k = keys[i];
+  if (!g.kb.real(k)) return;
+  const uint32_t x = g.kb.x_of(k), y = g.kb.y_of(k);
+  if (x >= y) return;
+  const uint64_t ek = edge_key(x, y, g.kb.c_of(k) % g.n_el);
+  if (del) edge_delete(g, ek); else edge_insert(g, ek);
+}
+
 // ------------------------------------------------- one update per launch
 //
 // The plain form runs each edge update on its own.  A batch of one needs no
@@ -619,6 +679,11 @@ __global__ void __launch_bounds__(256) k_plain_mutate(DevGraph g, const UpdInfo*
       }
       __syncthreads();
     }
+  }
+  if (g.emask && (inf.flags & UF_MUT) && lane == 0) {  // the edge table follows the rows
+    const uint64_t k0 = keys[0];
+    const uint64_t ek = edge_key(g.kb.x_of(k0), g.kb.y_of(k0), g.kb.c_of(k0) % g.n_el);
+    if (inf.flags & UF_ADD) edge_insert(g, ek); else edge_delete(g, ek);
   }
   if (out && lane == 0) {
     // an update whose label triple matches no query edge: nothing to count

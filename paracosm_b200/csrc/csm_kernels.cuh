@@ -51,6 +51,15 @@ void launch_mut_delete(const VRange* ranges, const unsigned int* n_ranges, const
                        cudaStream_t st);
 __global__ void k_vdel_keys(DevGraph g, uint32_t v, uint32_t deg, uint64_t* keys);
 
+// ---- edge table (csm_kernels.cu) ----
+// Inserts every (edge, label) of the CSR (one warp per row, from the row of
+// the smaller endpoint).
+__global__ void k_edge_fill(DevGraph g);
+// Inserts (del = 0) or deletes (del = 1) the edges of a packed-key list of
+// directed entries (x, combo, y) (the batch lists; each edge appears in both
+// directions and is taken from x < y).
+__global__ void k_edge_list(const uint64_t* keys, uint32_t L, DevGraph g, uint32_t del);
+
 // ---- one edge update per launch sequence (the plain form; csm_kernels.cu) ----
 // keys[0..1]: the update's two directed entries (sentinels when the graph does
 // not change); cnt[0..15], count/hash/bytes/stop[0]: cleared for the search.

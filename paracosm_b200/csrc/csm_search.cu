@@ -187,10 +187,53 @@ __device__ __forceinline__ bool check_candidate_q(const SearchParams& p, const u
   return true;
 }
 
+// The same check with the edge table (DevGraph::ekeys): each join is one
+// probe for the key of edge (m[b], x) with back entry b's edge label, the
+// first probes of four back entries issued together and in flight with the
+// candidate-filter word.  Most candidates fail a join (the join segments are
+// hub rows of hundreds to thousands of entries), and a probe settles it in
+// one round trip where a binary search needs one per halving.  The batch-time
+// presence of the back edges is tested for the candidates that pass.
+__device__ __forceinline__ bool check_candidate_h(const SearchParams& p, const PlanAnchor* A, uint32_t pos,
+                                                  uint32_t x, const uint32_t* m, uint32_t dsel, int32_t t,
+                                                  uint32_t lab_mask = 0xffffffffu) {
+  const PlanPos P = A->pos[pos];
+  const DevGraph& g = p.g;
+  const uint64_t fw = p.d2 ? p.d2[(uint64_t)P.qv * p.d2_words + (x >> 6)] : ~0ULL;
+  bool ok = true;
+  if (!p.homo) {
+    for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) ok &= m[__ffs(mk) - 1] != x;
+  }
+  if (!ok) return false;
+  for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
+    uint64_t key[4], slot[4], first[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b = b0 + (uint32_t)i;
+      key[i] = kEdgeEmpty; slot[i] = 0; first[i] = kEdgeEmpty;
+      if (b < P.nb && b != dsel) {
+        key[i] = edge_key(m[A->back_pos[P.boff + b]], x, A->back_combo[P.boff + b] % g.n_el);
+        slot[i] = edge_slot(key[i], g.emask);
+        first[i] = g.ekeys[slot[i]];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (key[i] != kEdgeEmpty && !edge_probe_rest(g, key[i], slot[i], first[i])) return false;
+  }
+  if (!((fw >> (x & 63)) & 1ULL)) return false;
+  for (uint32_t b = 0; b < P.nb; b++) {
+    const uint32_t v = m[A->back_pos[P.boff + b]];
+    if (g.t_count[v] && !present_at(g, v, A->back_combo[P.boff + b], x, t)) return false;
+  }
+  return true;
+}
+
 // The same check when no quad was prefetched.
 __device__ __forceinline__ bool check_candidate(const SearchParams& p, const uint32_t* pool, const PlanAnchor* A,
                                                 uint32_t pos, uint32_t x, const uint32_t* m, uint32_t dsel,
                                                 int32_t t, uint32_t lab_mask = 0xffffffffu) {
+  if (p.g.emask) return check_candidate_h(p, A, pos, x, m, dsel, t, lab_mask);
   SegQuad q0;
   load_quad(p.g, A, A->pos[pos], 0, m, dsel, q0);
   return check_candidate_q(p, pool, A, pos, x, m, dsel, t, q0, lab_mask);
@@ -623,9 +666,13 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
       uint32_t idx = e;
       for (int l2 = d; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
       const uint32_t ds = L.dsel[e];
-      SegQuad q0;
-      load_quad(p.g, A, A->pos[pos], 0, m, ds, q0);
-      valid = check_candidate_q(p, pool, A, pos, x, m, ds, (int32_t)t, q0);
+      if (p.g.emask) {
+        valid = check_candidate_h(p, A, pos, x, m, ds, (int32_t)t);
+      } else {
+        SegQuad q0;
+        load_quad(p.g, A, A->pos[pos], 0, m, ds, q0);
+        valid = check_candidate_q(p, pool, A, pos, x, m, ds, (int32_t)t, q0);
+      }
       if (valid && pos + 1 < n) {
         m[pos] = x;
         valid = pick_driver(p, A, pos + 1, m, (int32_t)t, ndlo, ndn, ndsel, nb4);
