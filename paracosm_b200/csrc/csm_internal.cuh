@@ -117,6 +117,21 @@ __device__ __forceinline__ uint64_t edge_slot(uint64_t key, uint64_t mask) {
   x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
   return x & mask;
 }
+// Loads of data read once per use at random places (edge-table slots, filter
+// words, driver segments): they may fill L1 but go first when L1 needs room,
+// so they do not push out the lines that are reused -- the search's register
+// spills and the plan.
+__device__ __forceinline__ uint64_t ld_stream(const uint64_t* a) {
+  uint64_t v;
+  asm("ld.global.L1::evict_first.u64 %0, [%1];" : "=l"(v) : "l"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* a) {
+  uint32_t v;
+  asm("ld.global.L1::evict_first.u32 %0, [%1];" : "=r"(v) : "l"(a));
+  return v;
+}
+
 // Probe sequence from a slot already loaded (first = ekeys[slot]).
 __device__ __forceinline__ bool edge_probe_rest(const DevGraph& g, uint64_t key, uint64_t slot, uint64_t first) {
   uint64_t k = first;
@@ -124,7 +139,7 @@ __device__ __forceinline__ bool edge_probe_rest(const DevGraph& g, uint64_t key,
     if (k == key) return true;
     if (k == kEdgeEmpty) return false;
     slot = (slot + 1) & g.emask;
-    k = g.ekeys[slot];
+    k = ld_stream(g.ekeys + slot);
   }
   return false;
 }

@@ -199,7 +199,7 @@ __device__ __forceinline__ bool check_candidate_h(const SearchParams& p, const P
                                                   uint32_t lab_mask = 0xffffffffu) {
   const PlanPos P = A->pos[pos];
   const DevGraph& g = p.g;
-  const uint64_t fw = p.d2 ? p.d2[(uint64_t)P.qv * p.d2_words + (x >> 6)] : ~0ULL;
+  const uint64_t fw = p.d2 ? ld_stream(p.d2 + (uint64_t)P.qv * p.d2_words + (x >> 6)) : ~0ULL;
   bool ok = true;
   if (!p.homo) {
     for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) ok &= m[__ffs(mk) - 1] != x;
@@ -214,7 +214,7 @@ __device__ __forceinline__ bool check_candidate_h(const SearchParams& p, const P
       if (b < P.nb && b != dsel) {
         key[i] = edge_key(m[A->back_pos[P.boff + b]], x, A->back_combo[P.boff + b] % g.n_el);
         slot[i] = edge_slot(key[i], g.emask);
-        first[i] = g.ekeys[slot[i]];
+        first[i] = ld_stream(g.ekeys + slot[i]);
       }
     }
 #pragma unroll
@@ -503,7 +503,7 @@ __device__ __forceinline__ bool tail_stage(const SearchParams& p, const uint32_t
         const uint32_t o_dsel = __shfl_sync(0xffffffffu, dsel, own);
         if (gidx < total) {
           const uint32_t kk = gidx - (owner ? prev : 0u);
-          const uint32_t x = pool[(uint64_t)o_dlo + kk];
+          const uint32_t x = ld_stream(pool + (uint64_t)o_dlo + kk);
           load_prefix(m, lv, L, ce + owner, m0, m1);
           if (check_candidate(p, pool, A, ps, x, m, o_dsel, (int32_t)t, pmask)) {
             uint32_t M = 1u << j;
@@ -608,8 +608,10 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     }
     // the stop flag and the idle-warp count the checks above read are loaded
     // one iteration ahead, so their round trip to L2 overlaps a step's work
-    // instead of preceding it (a step late is soon enough for both)
-    if (lane == 0) {
+    // instead of preceding it (a step late is soon enough for both), and only
+    // before the iterations that read them: each load is a round trip to a
+    // line other warps update
+    if (lane == 0 && (iter & 3) == 3) {
       seen_stop = stop[t];
       seen_hungry = p.dq ? *(volatile unsigned int*)&p.q->hungry : 0u;
     }
@@ -661,7 +663,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     if (act) {
       // the candidate and the first back segments of its position are loaded
       // together: the segments depend on the prefix only
-      x = pool[(uint64_t)L.dlo[e] + kk];
+      x = ld_stream(pool + (uint64_t)L.dlo[e] + kk);
       m[0] = m0; m[1] = m1;
       uint32_t idx = e;
       for (int l2 = d; l2 >= 2; --l2) { m[l2] = lv[l2].v[idx]; idx = lv[l2].par[idx]; }
