@@ -188,12 +188,14 @@ __device__ __forceinline__ bool check_candidate_q(const SearchParams& p, const u
 }
 
 // The same check with the edge table (DevGraph::ekeys): each join is one
-// probe for the key of edge (m[b], x) with back entry b's edge label, the
-// first probes of four back entries issued together and in flight with the
-// candidate-filter word.  Most candidates fail a join (the join segments are
-// hub rows of hundreds to thousands of entries), and a probe settles it in
-// one round trip where a binary search needs one per halving.  The batch-time
-// presence of the back edges is tested for the candidates that pass.
+// probe for the key of edge (m[b], x) with back entry b's edge label.  The
+// candidate-filter word comes first (the filter is small and stays in L2),
+// then the joins one at a time, stopping at the first that fails: the table
+// is larger than L2, every probe of it is a random line fetched from HBM, and
+// HBM is what bounds this search -- most candidates fail their first join,
+// and probing all back entries at once (four in flight) fetched three times
+// the lines for a candidate that one probe settles.  The batch-time presence
+// of the back edges is tested for the candidates that pass.
 __device__ __forceinline__ bool check_candidate_h(const SearchParams& p, const PlanAnchor* A, uint32_t pos,
                                                   uint32_t x, const uint32_t* m, uint32_t dsel, int32_t t,
                                                   uint32_t lab_mask = 0xffffffffu) {
@@ -205,23 +207,13 @@ __device__ __forceinline__ bool check_candidate_h(const SearchParams& p, const P
     for (uint32_t mk = P.samelab & lab_mask; mk; mk &= mk - 1) ok &= m[__ffs(mk) - 1] != x;
   }
   if (!ok) return false;
-  for (uint32_t b0 = 0; b0 < P.nb; b0 += 4) {
-    uint64_t key[4], slot[4], first[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const uint32_t b = b0 + (uint32_t)i;
-      key[i] = kEdgeEmpty; slot[i] = 0; first[i] = kEdgeEmpty;
-      if (b < P.nb && b != dsel) {
-        key[i] = edge_key(m[A->back_pos[P.boff + b]], x, A->back_combo[P.boff + b] % g.n_el);
-        slot[i] = edge_slot(key[i], g.emask);
-        first[i] = ld_stream(g.ekeys + slot[i]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-      if (key[i] != kEdgeEmpty && !edge_probe_rest(g, key[i], slot[i], first[i])) return false;
-  }
   if (!((fw >> (x & 63)) & 1ULL)) return false;
+  for (uint32_t b = 0; b < P.nb; b++) {
+    if (b == dsel) continue;
+    const uint64_t key = edge_key(m[A->back_pos[P.boff + b]], x, A->back_combo[P.boff + b] % g.n_el);
+    const uint64_t slot = edge_slot(key, g.emask);
+    if (!edge_probe_rest(g, key, slot, ld_stream(g.ekeys + slot))) return false;
+  }
   for (uint32_t b = 0; b < P.nb; b++) {
     const uint32_t v = m[A->back_pos[P.boff + b]];
     if (g.t_count[v] && !present_at(g, v, A->back_combo[P.boff + b], x, t)) return false;
