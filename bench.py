@@ -35,10 +35,10 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact counts"
-# DRAM bytes (read + write) of one search launch over a 4,096-update C3
+# DRAM bytes (read + write) of one search launch over a 16,384-update C3
 # batch, from an ncu capture of that launch (dram__bytes_read.sum +
 # dram__bytes_write.sum); scaled to a launch by the updates it processes.
-SEARCH_DRAM_BYTES_PER_4096 = 93.0e6
+SEARCH_DRAM_BYTES_PER_16384 = 47.6e9
 
 CONFIGS = {
     "c3": {
@@ -804,8 +804,8 @@ def main():
                     "counts_equal_device_resident": e2e_same},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None,
-                         "traffic": SEARCH_DRAM_BYTES_PER_4096 * B / 4096 if cfg["preset"] == "c3" else None,
-                         "traffic_note": "ncu dram__bytes_read+write of a 4096-update C3 launch, scaled by updates",
+                         "traffic": SEARCH_DRAM_BYTES_PER_16384 * B / 16384 if cfg["preset"] == "c3" else None,
+                         "traffic_note": "ncu dram__bytes_read+write of a 16384-update C3 launch, scaled by updates",
                          "peak_kind": peak_kind, "kernel": "k_search", "launches": search_n,
                          "kernel_ms": search_ms, "algorithmic_bytes": work},
             "cpu_baseline": cpu,
