@@ -924,6 +924,10 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
         const unsigned long long sv = *(volatile unsigned long long*)(p.qseq + (h & (p.qcap - 1)));
         if (sv == h + 1) {
           if (atomicCAS((unsigned long long*)&p.q->head, h, h + 1) == h) { claimed = h; seen = sv; break; }
+          // another warp took it: back off 32-287 ns (a per-warp spread) before
+          // the next try, so that a crowd of idle warps does not keep the
+          // head's line busy with failing compare-and-swaps
+          __nanosleep(32u + (((blockIdx.x * 32u + warp) * 2654435761u) >> 24));
           continue;
         }
         if (q->pending == 0) break;
