@@ -87,10 +87,13 @@ struct DTask {
 };
 static_assert(sizeof(DTask) == 160, "DTask is 160 bytes");
 
-// Work queue of the search launches.  Tickets (head, tail) count up across
-// launches; `pending` counts this launch's tasks (root and donated) that are
-// not finished, and idle warps exit when it reaches zero; `hungry` counts idle
-// warps not yet promised a task, which caps how much busy warps hand over.
+// Work queue of the search launches.  Tickets count up across launches: an
+// idle warp takes ticket `head` (fetch-and-add) and waits for its record; a
+// busy warp hands work over by filling tickets from `tail`, one per unit of
+// `hungry` it takes (a signed count of idle warps not yet promised a record),
+// so records go to waiting warps in ticket order and tail never passes head.
+// `pending` counts this launch's tasks (root and donated) that are not
+// finished, and waiting warps exit when it reaches zero.
 struct SearchQueue {
   unsigned long long head, tail;
   unsigned int hungry, pending;

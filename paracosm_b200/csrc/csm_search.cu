@@ -308,17 +308,16 @@ __device__ uint32_t donate(const SearchParams& p, LevelSM* lv, int d, uint32_t l
   LevelSM& S = lv[Ls];
   const uint32_t cnt = S.cnt, ce = S.cur_e;
   const uint32_t avail = mode == 1 ? min(cnt - ce - 1, 32u) : 1u;
-  // take up to `avail` units of hunger (idle warps not yet promised a task)
+  // take up to `avail` units of hunger (idle warps not yet promised a
+  // record; a signed count): one subtraction, the excess given back, no
+  // retries however many warps donate at once
   unsigned long long base = 0;
   uint32_t k = 0;
   if (lane == 0) {
-    unsigned int h = *(volatile unsigned int*)&p.q->hungry;
-    while (h) {
-      const unsigned int want = min(h, min(avail, idle_now));
-      const unsigned int prev = atomicCAS(&p.q->hungry, h, h - want);
-      if (prev == h) { k = want; break; }
-      h = prev;
-    }
+    const uint32_t want = min(avail, idle_now);
+    const int old = (int)atomicSub(&p.q->hungry, want);
+    k = old <= 0 ? 0u : min((uint32_t)old, want);
+    if (k < want) atomicAdd(&p.q->hungry, want - k);
     if (k) {
       atomicAdd(&p.q->pending, k);
       base = atomicAdd(&p.q->tail, (unsigned long long)k);
@@ -605,7 +604,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     // line other warps update
     if (lane == 0 && (iter & 3) == 3) {
       seen_stop = stop[t];
-      seen_hungry = p.dq ? *(volatile unsigned int*)&p.q->hungry : 0u;
+      seen_hungry = p.dq ? (uint32_t)max((int)*(volatile unsigned int*)&p.q->hungry, 0) : 0u;
     }
     if constexpr (MODE == 2) {
       if (d == tail_level) {
@@ -853,10 +852,13 @@ __device__ void run_donated(const SearchParams& p, const uint32_t* pool, LevelSM
 }
 
 // Per launch: tickets keep counting up across launches (the ring's slot
-// sequence numbers stay consistent); hunger and pending start afresh.
+// sequence numbers stay consistent); hunger and pending start afresh, and the
+// tickets that warps still waiting at the end of the last launch held (never
+// filled) are handed out again.
 __global__ void k_search_prep(SearchQueue* q, const unsigned int* n_tasks, uint32_t task_cap, SearchStats* ss,
                               unsigned int* error) {
-  if (q->head != q->tail) atomicExch(error, kErrRingState);  // an earlier launch left the ring undrained
+  if (q->head < q->tail) atomicExch(error, kErrRingState);
+  q->head = q->tail;  // tickets that waiting warps held when the last launch ended were never filled
   q->hungry = 0;
   q->pending = min(*n_tasks, task_cap);
   ss->launch_t0 = global_ns();
@@ -911,37 +913,26 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
   // 2. donated tasks until every task is done.  The queue is a bounded ring
   // of DTask slots with per-slot sequence numbers: slot (ticket % qcap) holds
   // ticket T's record once seq == T + 1, and is free for ticket T + qcap once
-  // its reader stores seq = T + qcap.
+  // its reader stores seq = T + qcap.  Claims take a ticket by fetch-and-add:
+  // a compare-and-swap on the head, retried by thousands of idle warps at
+  // once, took most of the warps' time late in a batch.
   volatile SearchQueue* q = p.q;
-  bool registered = false;
   for (;;) {
     unsigned long long claimed = ~0ULL, seen = 0;
     if (lane == 0) {
       const unsigned long long t0 = global_ns();
-      unsigned int nap = 64;
+      // this warp's ticket, and one unit of hunger for it: donors fill the
+      // tickets in order, one per unit they take
+      const unsigned long long tk = atomicAdd((unsigned long long*)&p.q->head, 1ull);
+      atomicAdd(&p.q->hungry, 1u);
+      unsigned int nap = 32;
       for (;;) {
-        const unsigned long long h = q->head;
-        const unsigned long long sv = *(volatile unsigned long long*)(p.qseq + (h & (p.qcap - 1)));
-        if (sv == h + 1) {
-          if (atomicCAS((unsigned long long*)&p.q->head, h, h + 1) == h) { claimed = h; seen = sv; break; }
-          // another warp took it: back off 32-287 ns (a per-warp spread) before
-          // the next try, so that a crowd of idle warps does not keep the
-          // head's line busy with failing compare-and-swaps
-          __nanosleep(32u + (((blockIdx.x * 32u + warp) * 2654435761u) >> 24));
-          continue;
-        }
+        const unsigned long long sv = *(volatile unsigned long long*)(p.qseq + (tk & (p.qcap - 1)));
+        if (sv == tk + 1) { claimed = tk; seen = sv; break; }
         if (q->pending == 0) break;
-        if (!registered) { atomicAdd(&p.q->hungry, 1u); registered = true; }
         __nanosleep(nap);
-        nap = min(nap * 2, 2048u);
+        nap = min(nap * 2, 1024u);
         if (global_ns() - t0 > p.wait_limit_ns) { atomicExch(p.error, kErrWaitTimeout); break; }
-      }
-      if (claimed != ~0ULL) {
-        // hungry = registered idle warps - published unclaimed tasks: a task taken
-        // by a warp that never registered was promised to a registered one, whose
-        // unit goes back into the count
-        if (!registered) atomicAdd(&p.q->hungry, 1u);
-        registered = false;
       }
       idle_ns += global_ns() - t0;
     }
