@@ -97,7 +97,7 @@ typedef struct csm_cfg {
                                  % shard_count == shard_rank; the per-update results of all shards sum
                                  to the unsharded ones (counts capped at max_results after the sum).
                                  shard_count 0 or 1: no sharding */
-  uint32_t donate_every;      /* search hand-over check interval in steps (power of two); 0 = autotuned / 4 */
+  uint32_t donate_every;      /* search hand-over check interval in steps (power of two); 0 = autotuned / 1 */
   uint32_t split_deep;        /* smallest driver range split deep in the search tree; 0 = autotuned / 64 */
   uint32_t enum_capacity;     /* > 0: keep up to this many embeddings of each submit (--print-enum,
                                  read with csm_gpu_matches); not with CSM_GRAPHS_ON */

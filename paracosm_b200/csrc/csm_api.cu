@@ -1105,10 +1105,10 @@ static int autotune(csm_ctx* ctx, uint32_t n, const csm_update* h_edges, uint32_
       if (ms < best && ms < 0.95f * def_ms) { best = ms; best_w = w; best_b = b; }
     }
   }
-  // hand-over settings for the chosen shape, against the default (4, 64)
+  // hand-over settings for the chosen shape, against the default (every step, 64)
   uint32_t best_every = 0, best_split = 0;
   const float shape_ms = best;
-  static const uint32_t kHandOver[4][2] = {{2u, 32u}, {8u, 128u}, {4u, 16u}, {16u, 256u}};
+  static const uint32_t kHandOver[4][2] = {{2u, 64u}, {4u, 64u}, {1u, 16u}, {1u, 256u}};
   for (const auto& cand : kHandOver) {
     rc = tune_run(ctx, B, best_w, best_b, &ms, cand[0], cand[1]);
     if (rc) return rc;

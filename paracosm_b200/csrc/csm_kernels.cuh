@@ -152,7 +152,7 @@ struct SearchParams {
   SearchStats* sstat;
   unsigned long long deadline_ns;  // per-update time budget from the launch's start; 0 = none
   // hand-over tuning: busy warps look for idle ones every donate_every
-  // iterations (a power of two; 0 = 4) and split a driver range deep in the
+  // iterations (a power of two; 0 = every iteration) and split a driver range deep in the
   // tree only when at least split_deep elements remain (0 = 64)
   uint32_t donate_every, split_deep;
   // match-set output (null: off): each embedding found at a leaf is appended

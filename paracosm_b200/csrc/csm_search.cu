@@ -591,7 +591,7 @@ __device__ void run_levels(const SearchParams& p, const uint32_t* pool, LevelSM*
     if ((iter & 7) == 0) {
       if (__shfl_sync(0xffffffffu, seen_stop, 0)) break;
     }
-    if ((iter & (p.donate_every ? p.donate_every - 1 : 3u)) == 0 && p.dq) {
+    if ((iter & (p.donate_every ? p.donate_every - 1 : 0u)) == 0 && p.dq) {
       const uint32_t idle_now = __shfl_sync(0xffffffffu, seen_hungry, 0);
       acc.checks++;
       if (idle_now) acc.checks_hungry++;
