@@ -38,7 +38,7 @@ METRIC = "updates/s, p50/p99 update latency: batched vs plain GPU, bit-exact cou
 # DRAM bytes (read + write) of one search launch over a 16,384-update C3
 # batch, from an ncu capture of that launch (dram__bytes_read.sum +
 # dram__bytes_write.sum); scaled to a launch by the updates it processes.
-SEARCH_DRAM_BYTES_PER_16384 = 47.6e9
+SEARCH_DRAM_BYTES_PER_16384 = 50.7e9
 
 CONFIGS = {
     "c3": {
