@@ -524,6 +524,10 @@ __device__ __forceinline__ void edge_delete(const DevGraph& g, uint64_t key) {
   }
 }
 
+// One warp per row: the lanes take the row's entries 32 at a time and find
+// each entry's combo by a binary search in the row's directory, so that a
+// row's insertions run side by side (combos hold a few entries each: looping
+// over combos left most lanes idle and the insertions one after another).
 __global__ void k_edge_fill(DevGraph g) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -531,14 +535,17 @@ __global__ void k_edge_fill(DevGraph g) {
   const uint32_t* pool = g.pools[g.ps->active];
   for (uint32_t v = warp; v < g.n; v += nwarps) {
     const uint32_t* dirv = g.dir + (size_t)v * (g.nc + 1);
-    if (dirv[g.nc] == 0) continue;
+    const uint32_t total = dirv[g.nc];
+    if (total == 0) continue;
     const uint64_t off = g.row_off[v];
-    for (uint32_t c = 0; c < g.nc; c++) {
-      const uint32_t lo = dirv[c], hi = dirv[c + 1];
-      for (uint32_t i = lo + lane; i < hi; i += 32) {
-        const uint32_t w = pool[off + i];
-        if (v < w) edge_insert(g, edge_key(v, w, c % g.n_el));
+    for (uint32_t i = lane; i < total; i += 32) {
+      uint32_t lo = 0, hi = g.nc - 1;  // the last combo c with dirv[c] <= i: its segment holds entry i
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (dirv[mid] <= i) lo = mid; else hi = mid - 1;
       }
+      const uint32_t w = pool[off + i];
+      if (v < w) edge_insert(g, edge_key(v, w, lo % g.n_el));
     }
   }
 }
