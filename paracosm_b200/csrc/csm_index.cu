@@ -598,18 +598,8 @@ int index_build(IndexState& ix, DevMem& mem, const DevGraph& g, const IndexQuery
   return rc;
 }
 
-int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,
-                      uint64_t* launches) {
-  if (!ix.active || L == 0) return CSM_OK;
-  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
-  k_ix_seed<<<(L + 255) / 256, 256, 0, st>>>(keys, L, g, ix.d_dag, ix.bits);
-  (*launches)++;
-  return index_launch_round(ix, g, st, launches, false);
-}
-
-int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys, cudaStream_t st,
-                         uint64_t* launches) {
-  if (!ix.active) return CSM_OK;
+// The incremental round as one cooperative launch (k_ix_round_coop).
+static int index_round_coop(IndexState& ix, const DevGraph& g, cudaStream_t st, uint64_t* launches) {
   if (!ix.coop_blocks) {
     int occ = 0;
     IXCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ix_round_coop, 256, 0));
@@ -617,9 +607,6 @@ int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys
     ix.coop_blocks = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>((warps_needed + 7) / 8, (uint64_t)ix.sm_count * (uint64_t)std::max(occ, 1)));
   }
-  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
-  k_ix_seed<<<1, 32, 0, st>>>(keys, 2, g, ix.d_dag, ix.bits);
-  (*launches)++;
   IxOrder ord{};
   ord.nq = ix.h_dag.nq;
   for (uint32_t i = 0; i < ord.nq; i++) ord.order[i] = ix.order[i];
@@ -630,6 +617,26 @@ int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys
   IXCK(cudaLaunchCooperativeKernel((const void*)k_ix_round_coop, dim3(ix.coop_blocks), dim3(256), args, 0, st));
   (*launches)++;
   return CSM_OK;
+}
+
+// A batch's changed edges: the seed over all of them, then the round in one
+// launch (2 |V_Q| + 1 launches per batch before).
+int index_apply_edges(IndexState& ix, const DevGraph& g, const uint64_t* keys, uint32_t L, cudaStream_t st,
+                      uint64_t* launches) {
+  if (!ix.active || L == 0) return CSM_OK;
+  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
+  k_ix_seed<<<(L + 255) / 256, 256, 0, st>>>(keys, L, g, ix.d_dag, ix.bits);
+  (*launches)++;
+  return index_round_coop(ix, g, st, launches);
+}
+
+int index_apply_edge_one(IndexState& ix, const DevGraph& g, const uint64_t* keys, cudaStream_t st,
+                         uint64_t* launches) {
+  if (!ix.active) return CSM_OK;
+  IXCK(cudaMemsetAsync(ix.bits.active, 0, 4, st));  // set by the seed when a changed entry matters
+  k_ix_seed<<<1, 32, 0, st>>>(keys, 2, g, ix.d_dag, ix.bits);
+  (*launches)++;
+  return index_round_coop(ix, g, st, launches);
 }
 
 int index_vertex_update(IndexState& ix, const DevGraph& g, const csm_update& h, cudaStream_t st, uint64_t* launches) {
